@@ -1,0 +1,329 @@
+#!/usr/bin/env python3
+"""Benchmark of the dense state-vector path on B200.
+
+Workload (one step): the reference's QFT circuit on n=28 qubits
+(circuit::appendQft: 28 H + 378 controlled phases + 14 swaps = 420 circuit
+ops) applied to the random-phase input of QuantumState::randomPhase(28,
+123456) in complex128 -- the plain FP64 form, bit-identical to the reference
+Dense backend.  Metric: amp-updates/s = circuit ops x 2^n per second of a
+step.  The 4 GiB state is larger than L2 (126 MB), so no flush is needed
+between steps.
+
+  value   device-resident: the state stays in HBM; each step applies the QFT
+          through tmfqs_gpu_apply_ops; timed with CUDA events on the handle's
+          stream, max over ranks.
+  e2e     the same metric through the C ABI with host buffers: each step
+          loads the input from pinned host memory, runs the QFT, and reads
+          back the exact total probability and a seeded measurement.
+  --impl reference   the reference's own Dense CPU path (oracle/_ref, compiled
+          from the reference sources) on this host, on a bounded prefix of the
+          same circuit.
+
+Multi-GPU: the path does not shard at this tier -- N ranks run N independent
+replicas ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "QFT/Grover amp-updates/s, %HBM peak: FP32-fused vs FP64-plain; adjoint grad/s"
+UNIT = "amp-updates/s"
+SEED = 123456
+REF_PREFIX_OPS = 8  # reference CPU sample: H(0) + 7 controlled phases of QFT-28 per step
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--qubits", type=int, default=28)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return rank, local, world
+
+
+def config(n):
+    return {
+        "workload": f"qft{n}_random_phase_c128_fp64_plain",
+        "n_qubits": n,
+        "circuit_ops": n + n * (n - 1) // 2 + n // 2,
+        "amplitude": "complex128",
+        "input": f"QuantumState::randomPhase({n}, {SEED}) (std::mt19937)",
+        "state_bytes": 16 << n,
+        "l2_policy": "inputs larger than L2 (state 4 GiB vs 126 MB L2); no flush needed",
+        "form": "fused passes, bit-identical to the reference Dense backend",
+    }
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(n):
+    """DRAM bytes per fused-pass launch from the committed ncu summary, scaled to 2^n."""
+    path = os.path.join(ROOT, "profiles", "fused_pass_qft_fp64.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["dram_bytes_per_launch"]) * (2.0 ** n) / (2.0 ** int(d["n_qubits"]))
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        load = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import tmfqsfullstate_b200 as tq
+
+    rank, local, world = dist_env()
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    n = args.qubits
+    N = 1 << n
+    ops = tq.qft_ops(n)
+    updates = len(ops) * N
+
+    host = torch.empty(2 * N, dtype=torch.float64, pin_memory=True)
+    inp = host.numpy()
+    tq.random_phase(n, SEED, inp)
+    rnd = float(tq.mt19937_unit(SEED, 1)[0])
+
+    g = tq.GpuState(tq.FP64, local)
+    g.load(n, inp)
+    stream = torch.cuda.ExternalStream(g.stream())
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        g.apply_ops(ops)
+    g.sync()
+    g.reset_stats()
+    g.set_option(tq.OPT_KERNEL_TIMING, 1)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        g.apply_ops(ops)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    stats = g.stats()
+    kt = g.kernel_times()
+    g.set_option(tq.OPT_KERNEL_TIMING, 0)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * updates * args.steps / (ms / 1e3)
+
+    # End to end through the C ABI with host buffers.
+    e2e_times = []
+    measured = total = None
+    for _ in range(max(1, args.e2e_steps)):
+        barrier()
+        t0 = time.perf_counter()
+        g.load(n, inp)
+        g.apply_ops(ops)
+        total = g.total_probability()
+        measured = g.sample(rnd)
+        t1 = time.perf_counter()
+        e2e_times.append(t1 - t0)
+    e2e_s = statistics.median(e2e_times)
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * updates / e2e_s
+
+    fused = kt["fused"]
+    peak, peak_kind = measured_peak_hbm()
+    roofline = None
+    if fused["launches"]:
+        bytes_per = fused["bytes"] / fused["launches"]
+        avg_ms = fused["ms"] / fused["launches"]
+        achieved = bytes_per / (avg_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": "k_fused<double> (fused multi-gate pass)", "achieved": achieved,
+                    "peak": peak, "peak_source": f"{peak_kind} hbm_gbs", "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": profiled_traffic(n), "bytes_per_launch": bytes_per, "avg_launch_ms": avg_ms,
+                    "share_of_step": fused["ms"] / ms if ms else None}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(n)
+
+    g.close()
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference random-phase input, seed 123456)",
+            "config": config(n), "parallelism": f"replicas x{world}",
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * N, "d2h_bytes_per_step": 16,
+                    "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": int(stats["kernel_launches"]),
+            "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+            "kernel_times_ms": {k: round(v["ms"], 3) for k, v in kt.items() if v["launches"]},
+            "check": {"total_probability": total, "measured": measured,
+                      "reference_golden": {"total_probability": 0.99999999999986022, "measured": 138222191}},
+        }
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def reference_sample(n, prefix_ops, steps, warmup):
+    """The reference Dense CPU path (oracle/_ref) on the first `prefix_ops` ops of QFT-n."""
+    import oracle as O
+
+    src = "reference" if O.ref_available() else "port"
+    ops = (O.ref_qft_ops(n) if src == "reference" else O.qft_ops(n))[:prefix_ops]
+    secs = []
+    if src == "reference":
+        st = O.RefState(n, "random_phase", seed=SEED)
+        for i in range(warmup + steps):
+            r = st.run(ops, want_amps=False)
+            if i >= warmup:
+                secs.append(r["seconds"])
+    else:
+        amps = O.random_phase(n, SEED)
+        for i in range(warmup + steps):
+            reg = O.OracleRegister(n, amps=amps)
+            t0 = time.perf_counter()
+            reg.run(ops)
+            if i >= warmup:
+                secs.append(time.perf_counter() - t0)
+    return src, secs, len(ops)
+
+
+def cpu_baseline(n):
+    src, secs, nops = reference_sample(n, REF_PREFIX_OPS, 1, 0)
+    v = nops * (1 << n) / statistics.median(secs)
+    return {"value": v, "unit": UNIT, "cores": 1, "kind": src,
+            "sample": f"first {nops} ops of QFT-{n} (H(0) + controlled phases) on the random-phase input, "
+                      f"reference Simulator executionSeconds, single-threaded Dense backend"}
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    n = args.qubits
+    try:
+        src, secs, nops = reference_sample(n, REF_PREFIX_OPS, args.steps, args.warmup)
+    except Exception as e:  # the reference could not run here
+        print(json.dumps({"impl": "reference", "unavailable": f"{type(e).__name__}: {e}"}))
+        return
+    s = statistics.median(secs)
+    value = nops * (1 << n) / s
+    cpu = {"value": value, "unit": UNIT, "cores": 1, "kind": src,
+           "sample": f"first {nops} ops of QFT-{n} per step on the random-phase input (reference Dense backend, "
+                     f"one thread; Simulator executionSeconds)"}
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference random-phase input, seed 123456)",
+        "config": config(n), "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,240 @@
+/*
+ * tmfqs_b200 -- C ABI of the B200 dense state-vector engine for TMFQS.
+ *
+ * One handle = one register's state vector resident in HBM plus the CUDA
+ * stream its kernels run on.  The C++ `gpu` storage strategy
+ * (GpuStateBackend, an IStateBackend) binds to these entry points; so do the
+ * Python tests and the benchmark.  Plain pointers and sizes only; host
+ * buffers are caller-owned; every call returns a tmfqs_status and leaves a
+ * message for tmfqs_gpu_last_error() on failure.
+ *
+ * Layout in HBM: 2^n interleaved complex amplitudes [re0, im0, re1, im1, ...]
+ * -- complex128 (TMFQS_FP64, the reference's AmplitudesVector layout,
+ * include/tmfqs/core/types.h:28) or complex64 (TMFQS_FP32).  Qubit q is bit
+ * (n-1-q) of the state index (qubit 0 = most significant, types.h:12-13).
+ *
+ * Semantics follow the reference Dense backend operation by operation.  In
+ * TMFQS_FP64 every gate, diffusion, affine map, total probability and
+ * measurement is bit-identical to the reference (same IEEE operations in the
+ * same order; sequential sums replayed exactly).  Reference citations below
+ * are paths inside the reference project.
+ */
+#ifndef TMFQS_B200_H
+#define TMFQS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define TMFQS_API __attribute__((visibility("default")))
+#else
+#define TMFQS_API
+#endif
+
+typedef struct tmfqs_gpu_state tmfqs_gpu_state;
+
+/* Status codes; each maps to the exception class the reference throws. */
+typedef enum {
+	TMFQS_OK = 0,
+	TMFQS_ERR_OUT_OF_RANGE = 1,    /* std::out_of_range   (validation.h:19-41) */
+	TMFQS_ERR_INVALID_ARGUMENT = 2, /* std::invalid_argument (validation.h:43-80) */
+	TMFQS_ERR_LOGIC = 3,           /* std::logic_error (backend_validation.h:13-18) */
+	TMFQS_ERR_RUNTIME = 4,         /* std::runtime_error (dense_state_backend.cpp:186) */
+	TMFQS_ERR_CUDA = 5,            /* CUDA failure (mapped to std::runtime_error) */
+	TMFQS_ERR_NOMEM = 6            /* device allocation failure (std::runtime_error) */
+} tmfqs_status;
+
+typedef enum {
+	TMFQS_FP64 = 0, /* complex128 amplitudes, FP64 arithmetic (plain form) */
+	TMFQS_FP32 = 1  /* complex64 amplitudes, FP32 gates, FP64 reductions (precision form) */
+} tmfqs_precision;
+
+/* Circuit operation: the circuit::Operation variant (circuit/circuit.h:16-61). */
+typedef enum {
+	TMFQS_OP_H = 0,          /* Hadamard{target}                 */
+	TMFQS_OP_X = 1,          /* PauliX{target}                   */
+	TMFQS_OP_CNOT = 2,       /* ControlledNot{control, target}   */
+	TMFQS_OP_CPHASE = 3,     /* ControlledPhaseShift{c, t, theta} */
+	TMFQS_OP_SWAP = 4,       /* Swap{first, second}              */
+	TMFQS_OP_GATE = 5,       /* MatrixGate{gate, targets}        */
+	TMFQS_OP_PHASE_FLIP = 6, /* PhaseFlipBasisState{state}       */
+	TMFQS_OP_INVERSION = 7   /* InversionAboutMean{materialized} */
+} tmfqs_op_kind;
+
+typedef struct {
+	int kind;               /* tmfqs_op_kind */
+	unsigned q0;            /* target (H, X); control (CNOT, CPHASE); first (SWAP) */
+	unsigned q1;            /* target (CNOT, CPHASE); second (SWAP) */
+	double theta;           /* CPHASE angle in radians */
+	uint64_t state;         /* PHASE_FLIP basis state */
+	int materialized;       /* INVERSION: 1 materialised, 0 lazy overlay */
+	const double *matrix;   /* GATE: row-major 2^k x 2^k interleaved complex (host) */
+	const unsigned *qubits; /* GATE: targets, first = most significant block bit */
+	unsigned k;             /* GATE: number of targets */
+} tmfqs_op;
+
+/* The register-side state that QuantumRegister keeps around its backend:
+ * cached logical amplitude sum and lazy affine overlay
+ * (register/quantum_register.h:218-224). */
+typedef struct {
+	int has_sum;
+	double sum_re, sum_im;
+	int overlay;
+	double scale_re, scale_im;
+	double bias_re, bias_im;
+} tmfqs_register_view;
+
+/* Counters of the work a handle has issued (for benchmarks and tests). */
+typedef struct {
+	uint64_t kernel_launches;   /* kernels launched by this handle */
+	uint64_t fused_passes;      /* fused multi-gate passes over the state */
+	uint64_t gate_passes;       /* single-gate passes over the state */
+	uint64_t reduction_passes;  /* passes of the exact reductions */
+	uint64_t h2d_bytes, d2h_bytes;
+} tmfqs_stats;
+
+/* Tunables (tmfqs_gpu_set_option). */
+typedef enum {
+	TMFQS_OPT_FUSION = 0,        /* 1 (default): apply_ops fuses gates into multi-gate passes */
+	TMFQS_OPT_FUSED_QUBITS = 1,  /* target qubits per fused pass (default 9) */
+	TMFQS_OPT_GROVER_FUSION = 2, /* 1 (default): Grover runs execute as one temporal pass */
+	TMFQS_OPT_KERNEL_TIMING = 3  /* 1: time every pass with CUDA events on the handle's stream */
+} tmfqs_option;
+
+/* Kernel classes for tmfqs_gpu_kernel_times. */
+typedef enum {
+	TMFQS_KT_FUSED = 0,   /* fused multi-gate pass */
+	TMFQS_KT_PERMUTE = 1, /* bit-permutation (swap run) pass */
+	TMFQS_KT_GATE = 2,    /* single-gate pass (incl. diffusion and affine sweeps) */
+	TMFQS_KT_REDUCE = 3,  /* exact reduction (sum, norm, measurement) */
+	TMFQS_KT_GROVER = 4,  /* temporal Grover pass */
+	TMFQS_KT_COUNT = 5
+} tmfqs_kernel_class;
+
+/* Accumulated device time of one kernel class since the last reset:
+ * launches, milliseconds (CUDA events), and algorithmic HBM bytes
+ * (one read + one write of the state per pass; reads only for reductions). */
+typedef struct {
+	uint64_t launches;
+	double ms;
+	double bytes;
+} tmfqs_kernel_time;
+
+/* ---- lifetime --------------------------------------------------------- */
+/* Creates an empty handle on `device` (no state yet). */
+TMFQS_API int tmfqs_gpu_create(int precision, int device, tmfqs_gpu_state **out);
+TMFQS_API int tmfqs_gpu_destroy(tmfqs_gpu_state *h);
+/* Deep copy: IStateBackend::clone, storage/i_state_backend.h:31. */
+TMFQS_API int tmfqs_gpu_clone(tmfqs_gpu_state *h, tmfqs_gpu_state **out);
+TMFQS_API const char *tmfqs_gpu_last_error(void);
+
+/* ---- initialisation / IO (storage/i_state_backend.h:37-66) ------------ */
+/* initZero, i_state_backend.h:37; dense_state_backend.cpp:77-81. */
+TMFQS_API int tmfqs_gpu_init_zero(tmfqs_gpu_state *h, unsigned num_qubits);
+/* initBasis, i_state_backend.h:44; dense_state_backend.cpp:84-89. */
+TMFQS_API int tmfqs_gpu_init_basis(tmfqs_gpu_state *h, unsigned num_qubits, uint64_t state, double re, double im);
+/* initUniformSuperposition, i_state_backend.h:50; dense_state_backend.cpp:92-115
+ * (deduplicates, amplitude 1/sqrt(unique count)). */
+TMFQS_API int tmfqs_gpu_init_uniform(tmfqs_gpu_state *h, unsigned num_qubits, const uint64_t *states, size_t count);
+/* loadAmplitudes, i_state_backend.h:56: 2^(n+1) doubles from host memory. */
+TMFQS_API int tmfqs_gpu_load(tmfqs_gpu_state *h, unsigned num_qubits, const double *host_amps);
+/* Loads `count` amplitudes starting at `first_state` into an initialised state. */
+TMFQS_API int tmfqs_gpu_load_chunk(tmfqs_gpu_state *h, uint64_t first_state, const double *host_amps, uint64_t count);
+/* exportAmplitudes, i_state_backend.h:61. */
+TMFQS_API int tmfqs_gpu_export(tmfqs_gpu_state *h, double *host_out);
+/* forEachAmplitudeChunk, i_state_backend.h:66: one chunk into a host buffer. */
+TMFQS_API int tmfqs_gpu_export_chunk(tmfqs_gpu_state *h, uint64_t first_state, double *host_out, uint64_t count);
+/* amplitude / setAmplitude, i_state_backend.h:73,79 (host-cached single reads/writes). */
+TMFQS_API int tmfqs_gpu_get_amp(tmfqs_gpu_state *h, uint64_t state, double *re, double *im);
+TMFQS_API int tmfqs_gpu_set_amp(tmfqs_gpu_state *h, uint64_t state, double re, double im);
+TMFQS_API int tmfqs_gpu_num_qubits(tmfqs_gpu_state *h, unsigned *out);
+TMFQS_API int tmfqs_gpu_precision(tmfqs_gpu_state *h, int *out);
+
+/* ---- reductions (bit-identical to the reference's sequential loops) --- */
+/* totalProbability, i_state_backend.h:90; dense_state_backend.cpp:161-171. */
+TMFQS_API int tmfqs_gpu_total_probability(tmfqs_gpu_state *h, double *out);
+/* sampleMeasurement, i_state_backend.h:96; dense_state_backend.cpp:173-188:
+ * first state whose running probability reaches rnd; rnd in [0,1). */
+TMFQS_API int tmfqs_gpu_sample(tmfqs_gpu_state *h, double rnd, uint64_t *out);
+/* Sequential sum of amplitudes (real and imaginary parts), the loop in
+ * QuantumRegister::logicalAmplitudeSum, quantum_register.cpp:176-190, and in
+ * inversionAboutMean(), dense_state_backend.cpp:213-228. */
+TMFQS_API int tmfqs_gpu_amplitude_sum(tmfqs_gpu_state *h, double *re, double *im);
+/* The same three reductions over logical amplitudes scale*a+bias
+ * (QuantumRegister overlay branches, quantum_register.cpp:160-165,176-211,269-310). */
+TMFQS_API int tmfqs_gpu_overlay_sum(tmfqs_gpu_state *h, double sre, double sim, double bre, double bim,
+                                    double *re, double *im);
+TMFQS_API int tmfqs_gpu_overlay_total_probability(tmfqs_gpu_state *h, double sre, double sim, double bre,
+                                                  double bim, double *out);
+TMFQS_API int tmfqs_gpu_overlay_sample(tmfqs_gpu_state *h, double sre, double sim, double bre, double bim,
+                                       double rnd, uint64_t *out);
+
+/* ---- single operations (storage/i_state_backend.h:104-151) ------------ */
+/* phaseFlipBasisState, i_state_backend.h:108; dense_state_backend.cpp:205-211. */
+TMFQS_API int tmfqs_gpu_phase_flip(tmfqs_gpu_state *h, uint64_t state);
+/* inversionAboutMean(), i_state_backend.h:110; dense_state_backend.cpp:213-228. */
+TMFQS_API int tmfqs_gpu_inversion(tmfqs_gpu_state *h);
+/* inversionAboutMean(mean), i_state_backend.h:115; dense_state_backend.cpp:230-240. */
+TMFQS_API int tmfqs_gpu_inversion_mean(tmfqs_gpu_state *h, double re, double im);
+/* applyAffineTransform, i_state_backend.h:121; dense_state_backend.cpp:242-253. */
+TMFQS_API int tmfqs_gpu_affine(tmfqs_gpu_state *h, double sre, double sim, double bre, double bim);
+/* applyHadamard, i_state_backend.h:126; dense_state_backend.cpp:255-274. */
+TMFQS_API int tmfqs_gpu_h(tmfqs_gpu_state *h, unsigned qubit);
+/* applyPauliX, i_state_backend.h:131; dense_state_backend.cpp:276-287. */
+TMFQS_API int tmfqs_gpu_x(tmfqs_gpu_state *h, unsigned qubit);
+/* applyControlledPhaseShift, i_state_backend.h:138; dense_state_backend.cpp:289-304
+ * (cos/sin of theta taken on the host with the C library, as the reference does). */
+TMFQS_API int tmfqs_gpu_cphase(tmfqs_gpu_state *h, unsigned control, unsigned target, double theta);
+/* applyControlledNot, i_state_backend.h:144; dense_state_backend.cpp:306-319. */
+TMFQS_API int tmfqs_gpu_cnot(tmfqs_gpu_state *h, unsigned control, unsigned target);
+/* applyGate, i_state_backend.h:151; gate_block_apply.h:103-213 (k <= 10). */
+TMFQS_API int tmfqs_gpu_gate(tmfqs_gpu_state *h, const double *matrix, const unsigned *qubits, unsigned k);
+/* QuantumRegister::applySwap, quantum_register.cpp:518-527, as one pass. */
+TMFQS_API int tmfqs_gpu_swap(tmfqs_gpu_state *h, unsigned a, unsigned b);
+
+/* ---- batched execution (sim::Simulator::run, simulator.cpp:54-96) ----- */
+/* Applies a run of gate operations (H, X, CNOT, CPHASE, SWAP, GATE,
+ * PHASE_FLIP) with register semantics, fusing them into multi-gate passes
+ * over HBM.  INVERSION is rejected here: it depends on register state and
+ * goes through tmfqs_gpu_grover_run or the single-op entry points. */
+TMFQS_API int tmfqs_gpu_apply_ops(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count);
+/* Runs `iterations` Grover iterations -- a phase flip of each sorted, unique
+ * marked state, then inversion about the mean, materialised or lazy -- with
+ * exactly the register semantics of QuantumRegister::applyPhaseFlipBasisState
+ * and applyInversionAboutMean[Materialized] (quantum_register.cpp:405-467),
+ * updating *view in place (appendGrover, circuit.cpp:118-141). */
+TMFQS_API int tmfqs_gpu_grover_run(tmfqs_gpu_state *h, tmfqs_register_view *view, const uint64_t *marked,
+                                   size_t count, uint64_t iterations, int materialized);
+/* endOperationBatch, i_state_backend.h:163: waits for all queued work. */
+TMFQS_API int tmfqs_gpu_sync(tmfqs_gpu_state *h);
+
+/* ---- host-side inputs and draws (no GPU needed) ------------------------ */
+/* QuantumState::randomPhase(n, seed), state/quantum_state.cpp:264-277 (and
+ * buildRandomPhaseInput, examples/qftG.cpp:70-81): 2^(n+1) doubles. */
+TMFQS_API int tmfqs_random_phase(unsigned num_qubits, uint32_t seed, double *host_out);
+/* The first `count` draws of Mt19937RandomSource(seed).nextUnitDouble(),
+ * core/random.h:32-58 -- the draws measure() consumes. */
+TMFQS_API int tmfqs_mt19937_unit(uint32_t seed, uint64_t count, double *host_out);
+
+/* ---- instrumentation -------------------------------------------------- */
+TMFQS_API int tmfqs_gpu_stats(tmfqs_gpu_state *h, tmfqs_stats *out);
+TMFQS_API int tmfqs_gpu_reset_stats(tmfqs_gpu_state *h);
+TMFQS_API int tmfqs_gpu_set_option(tmfqs_gpu_state *h, int option, long value);
+/* Per-class device times recorded while TMFQS_OPT_KERNEL_TIMING is on
+ * (synchronises the stream; `out` has TMFQS_KT_COUNT entries).  Reset with
+ * tmfqs_gpu_reset_stats. */
+TMFQS_API int tmfqs_gpu_kernel_times(tmfqs_gpu_state *h, tmfqs_kernel_time *out);
+/* The handle's device buffer and CUDA stream (for device-resident benchmarks
+ * and interop; the buffer stays owned by the handle). */
+TMFQS_API int tmfqs_gpu_device_buffer(tmfqs_gpu_state *h, void **ptr, size_t *bytes);
+TMFQS_API int tmfqs_gpu_stream(tmfqs_gpu_state *h, void **stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TMFQS_B200_H */

@@ -1,0 +1,460 @@
+"""tmfqsfullstate_b200 -- B200 dense state-vector engine for TMFQS.
+
+The product is native: ``libtmfqs_b200.so`` (hand-written sm_100a CUDA
+kernels behind the C ABI in ``include/tmfqs_b200.h``) and the C++17 host
+library that mirrors the reference's ``tmfqs::`` API on top of it
+(``host/``: ``QuantumRegister``, ``circuit::Circuit``, ``sim::Simulator`` with
+the ``gpu`` storage strategy, and the ``grover``/``groverLazy``/``qftG``
+CLIs).  This module is a thin ``ctypes`` binding of the C ABI, used by the
+tests, the smoke check and the benchmark.  There is no CPU fallback: if the
+shared library is missing or no GPU is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtmfqs_b200.so")
+HOST_LIB_PATH = os.path.join(HERE, "host", "libtmfqs.so")
+BIN_DIR = os.path.join(HERE, "host", "bin")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "tmfqs_b200.h")
+
+FP64, FP32 = 0, 1
+OP_H, OP_X, OP_CNOT, OP_CPHASE, OP_SWAP, OP_GATE, OP_PHASE_FLIP, OP_INVERSION = range(8)
+OPT_FUSION, OPT_FUSED_QUBITS, OPT_GROVER_FUSION = range(3)
+
+
+class TmfqsError(RuntimeError):
+    """A failed C-ABI call; ``status`` is the tmfqs_status code."""
+
+    status = 0
+
+
+class OutOfRange(TmfqsError, IndexError):
+    status = 1
+
+
+class InvalidArgument(TmfqsError, ValueError):
+    status = 2
+
+
+class LogicError(TmfqsError):
+    status = 3
+
+
+class RuntimeFailure(TmfqsError):
+    status = 4
+
+
+class CudaError(TmfqsError):
+    status = 5
+
+
+class DeviceOutOfMemory(TmfqsError, MemoryError):
+    status = 6
+
+
+_ERRORS = {c.status: c for c in (OutOfRange, InvalidArgument, LogicError, RuntimeFailure, CudaError, DeviceOutOfMemory)}
+
+
+class Op(ctypes.Structure):
+    """tmfqs_op (include/tmfqs_b200.h)."""
+
+    _fields_ = [
+        ("kind", ctypes.c_int),
+        ("q0", ctypes.c_uint),
+        ("q1", ctypes.c_uint),
+        ("theta", ctypes.c_double),
+        ("state", ctypes.c_uint64),
+        ("materialized", ctypes.c_int),
+        ("matrix", ctypes.POINTER(ctypes.c_double)),
+        ("qubits", ctypes.POINTER(ctypes.c_uint)),
+        ("k", ctypes.c_uint),
+    ]
+
+
+class RegisterView(ctypes.Structure):
+    """tmfqs_register_view: QuantumRegister's cached sum and affine overlay."""
+
+    _fields_ = [
+        ("has_sum", ctypes.c_int),
+        ("sum_re", ctypes.c_double),
+        ("sum_im", ctypes.c_double),
+        ("overlay", ctypes.c_int),
+        ("scale_re", ctypes.c_double),
+        ("scale_im", ctypes.c_double),
+        ("bias_re", ctypes.c_double),
+        ("bias_im", ctypes.c_double),
+    ]
+
+    @classmethod
+    def fresh(cls):
+        return cls(0, 0.0, 0.0, 0, 1.0, 0.0, 0.0, 0.0)
+
+
+class KernelTime(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_uint64), ("ms", ctypes.c_double), ("bytes", ctypes.c_double)]
+
+
+KT_NAMES = ("fused", "permute", "gate", "reduce", "grover")
+OPT_KERNEL_TIMING = 3
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("kernel_launches", ctypes.c_uint64),
+        ("fused_passes", ctypes.c_uint64),
+        ("gate_passes", ctypes.c_uint64),
+        ("reduction_passes", ctypes.c_uint64),
+        ("h2d_bytes", ctypes.c_uint64),
+        ("d2h_bytes", ctypes.c_uint64),
+    ]
+
+
+# Every entry point declared in include/tmfqs_b200.h, with its signature.
+_H = ctypes.c_void_p
+_D = ctypes.c_double
+_DP = ctypes.POINTER(ctypes.c_double)
+_U64 = ctypes.c_uint64
+_U64P = ctypes.POINTER(ctypes.c_uint64)
+_UI = ctypes.c_uint
+SIGNATURES = {
+    "tmfqs_gpu_create": [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_H)],
+    "tmfqs_gpu_destroy": [_H],
+    "tmfqs_gpu_clone": [_H, ctypes.POINTER(_H)],
+    "tmfqs_gpu_last_error": None,
+    "tmfqs_gpu_init_zero": [_H, _UI],
+    "tmfqs_gpu_init_basis": [_H, _UI, _U64, _D, _D],
+    "tmfqs_gpu_init_uniform": [_H, _UI, _U64P, ctypes.c_size_t],
+    "tmfqs_gpu_load": [_H, _UI, _DP],
+    "tmfqs_gpu_load_chunk": [_H, _U64, _DP, _U64],
+    "tmfqs_gpu_export": [_H, _DP],
+    "tmfqs_gpu_export_chunk": [_H, _U64, _DP, _U64],
+    "tmfqs_gpu_get_amp": [_H, _U64, _DP, _DP],
+    "tmfqs_gpu_set_amp": [_H, _U64, _D, _D],
+    "tmfqs_gpu_num_qubits": [_H, ctypes.POINTER(_UI)],
+    "tmfqs_gpu_precision": [_H, ctypes.POINTER(ctypes.c_int)],
+    "tmfqs_gpu_total_probability": [_H, _DP],
+    "tmfqs_gpu_sample": [_H, _D, _U64P],
+    "tmfqs_gpu_amplitude_sum": [_H, _DP, _DP],
+    "tmfqs_gpu_overlay_sum": [_H, _D, _D, _D, _D, _DP, _DP],
+    "tmfqs_gpu_overlay_total_probability": [_H, _D, _D, _D, _D, _DP],
+    "tmfqs_gpu_overlay_sample": [_H, _D, _D, _D, _D, _D, _U64P],
+    "tmfqs_gpu_phase_flip": [_H, _U64],
+    "tmfqs_gpu_inversion": [_H],
+    "tmfqs_gpu_inversion_mean": [_H, _D, _D],
+    "tmfqs_gpu_affine": [_H, _D, _D, _D, _D],
+    "tmfqs_gpu_h": [_H, _UI],
+    "tmfqs_gpu_x": [_H, _UI],
+    "tmfqs_gpu_cphase": [_H, _UI, _UI, _D],
+    "tmfqs_gpu_cnot": [_H, _UI, _UI],
+    "tmfqs_gpu_gate": [_H, _DP, ctypes.POINTER(_UI), _UI],
+    "tmfqs_gpu_swap": [_H, _UI, _UI],
+    "tmfqs_gpu_apply_ops": [_H, ctypes.POINTER(Op), ctypes.c_size_t],
+    "tmfqs_gpu_grover_run": [_H, ctypes.POINTER(RegisterView), _U64P, ctypes.c_size_t, _U64, ctypes.c_int],
+    "tmfqs_gpu_sync": [_H],
+    "tmfqs_gpu_stats": [_H, ctypes.POINTER(Stats)],
+    "tmfqs_gpu_reset_stats": [_H],
+    "tmfqs_gpu_set_option": [_H, ctypes.c_int, ctypes.c_long],
+    "tmfqs_gpu_kernel_times": [_H, ctypes.POINTER(KernelTime)],
+    "tmfqs_gpu_device_buffer": [_H, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)],
+    "tmfqs_gpu_stream": [_H, ctypes.POINTER(ctypes.c_void_p)],
+    "tmfqs_random_phase": [_UI, ctypes.c_uint32, _DP],
+    "tmfqs_mt19937_unit": [ctypes.c_uint32, _U64, _DP],
+}
+
+_lib = None
+
+
+def build(jobs: int = 8) -> None:
+    """Compile libtmfqs_b200.so and the C++ host library for sm_100a, in-tree."""
+    subprocess.run(["make", "-s", "-C", HERE, f"-j{jobs}"], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(HERE, "host"), f"-j{jobs}"], check=True)
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded C ABI.  Raises if the library was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` (no CPU fallback exists)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            if name == "tmfqs_gpu_last_error":
+                f.restype = ctypes.c_char_p
+                f.argtypes = []
+            else:
+                f.restype = ctypes.c_int
+                f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc:
+        msg = lib().tmfqs_gpu_last_error().decode(errors="replace")
+        raise _ERRORS.get(rc, TmfqsError)(msg)
+
+
+def _dptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise ValueError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_DP)
+
+
+# ---- op constructors -------------------------------------------------------
+
+def h(q):
+    return Op(kind=OP_H, q0=q)
+
+
+def x(q):
+    return Op(kind=OP_X, q0=q)
+
+
+def cnot(c, t):
+    return Op(kind=OP_CNOT, q0=c, q1=t)
+
+
+def cphase(c, t, theta):
+    return Op(kind=OP_CPHASE, q0=c, q1=t, theta=theta)
+
+
+def swap(a, b):
+    return Op(kind=OP_SWAP, q0=a, q1=b)
+
+
+def phase_flip(s):
+    return Op(kind=OP_PHASE_FLIP, state=s)
+
+
+def gate(matrix: np.ndarray, qubits):
+    m = np.ascontiguousarray(np.stack([np.real(matrix), np.imag(matrix)], axis=-1).reshape(-1), dtype=np.float64)
+    q = (ctypes.c_uint * max(1, len(qubits)))(*qubits)
+    op = Op(kind=OP_GATE, matrix=_dptr(m), qubits=ctypes.cast(q, ctypes.POINTER(ctypes.c_uint)), k=len(qubits))
+    op._buffers = (m, q)  # keep alive
+    return op
+
+
+PI = 3.14159265358979323846  # kPi (reference include/tmfqs/core/constants.h:6)
+
+
+def qft_ops(n: int):
+    """circuit::appendQft (reference src/tmfqs/circuit/circuit.cpp:87-100)."""
+    ops = []
+    for t in range(n):
+        ops.append(h(t))
+        for c in range(t + 1, n):
+            ops.append(cphase(c, t, PI / float(1 << (c - t))))
+    for l in range(n // 2):
+        ops.append(swap(l, n - l - 1))
+    return ops
+
+
+def random_phase(n: int, seed: int, out: np.ndarray | None = None) -> np.ndarray:
+    """QuantumState::randomPhase(n, seed) input (host, std::mt19937)."""
+    if out is None:
+        out = np.empty(2 << n, dtype=np.float64)
+    _check(lib().tmfqs_random_phase(n, seed, _dptr(out)))
+    return out
+
+
+def mt19937_unit(seed: int, count: int) -> np.ndarray:
+    """Mt19937RandomSource(seed).nextUnitDouble() draws."""
+    out = np.empty(count, dtype=np.float64)
+    _check(lib().tmfqs_mt19937_unit(seed, count, _dptr(out)))
+    return out
+
+
+def op_array(ops):
+    arr = (Op * max(1, len(ops)))()
+    for i, op in enumerate(ops):
+        arr[i] = op
+    arr._keep = list(ops)
+    return arr
+
+
+class GpuState:
+    """One register's state vector in HBM (a tmfqs_gpu_state handle)."""
+
+    def __init__(self, precision: int = FP64, device: int = 0, _handle=None):
+        self._h = ctypes.c_void_p()
+        if _handle is not None:
+            self._h = _handle
+        else:
+            _check(lib().tmfqs_gpu_create(precision, device, ctypes.byref(self._h)))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().tmfqs_gpu_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- lifetime / IO --
+    def clone(self) -> "GpuState":
+        out = ctypes.c_void_p()
+        _check(lib().tmfqs_gpu_clone(self._h, ctypes.byref(out)))
+        return GpuState(_handle=out)
+
+    @property
+    def num_qubits(self) -> int:
+        v = ctypes.c_uint()
+        _check(lib().tmfqs_gpu_num_qubits(self._h, ctypes.byref(v)))
+        return v.value
+
+    def init_zero(self, n):
+        _check(lib().tmfqs_gpu_init_zero(self._h, n))
+
+    def init_basis(self, n, s=0, amp=(1.0, 0.0)):
+        _check(lib().tmfqs_gpu_init_basis(self._h, n, s, amp[0], amp[1]))
+
+    def init_uniform(self, n, states):
+        a = np.ascontiguousarray(np.array(states, dtype=np.uint64))
+        _check(lib().tmfqs_gpu_init_uniform(self._h, n, a.ctypes.data_as(_U64P), len(a)))
+
+    def load(self, n, amps: np.ndarray):
+        a = np.ascontiguousarray(amps, dtype=np.float64)
+        if a.size != 2 << n:
+            raise ValueError("amplitude buffer size mismatch")
+        _check(lib().tmfqs_gpu_load(self._h, n, _dptr(a)))
+
+    def load_chunk(self, first, amps: np.ndarray):
+        a = np.ascontiguousarray(amps, dtype=np.float64)
+        _check(lib().tmfqs_gpu_load_chunk(self._h, first, _dptr(a), a.size // 2))
+
+    def export(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(2 << self.num_qubits, dtype=np.float64)
+        _check(lib().tmfqs_gpu_export(self._h, _dptr(out)))
+        return out
+
+    def export_chunk(self, first, count) -> np.ndarray:
+        out = np.empty(2 * count, dtype=np.float64)
+        _check(lib().tmfqs_gpu_export_chunk(self._h, first, _dptr(out), count))
+        return out
+
+    def amplitude(self, s):
+        re, im = ctypes.c_double(), ctypes.c_double()
+        _check(lib().tmfqs_gpu_get_amp(self._h, s, ctypes.byref(re), ctypes.byref(im)))
+        return re.value, im.value
+
+    def set_amplitude(self, s, re, im):
+        _check(lib().tmfqs_gpu_set_amp(self._h, s, re, im))
+
+    # -- reductions --
+    def total_probability(self) -> float:
+        v = ctypes.c_double()
+        _check(lib().tmfqs_gpu_total_probability(self._h, ctypes.byref(v)))
+        return v.value
+
+    def sample(self, rnd: float) -> int:
+        v = ctypes.c_uint64()
+        _check(lib().tmfqs_gpu_sample(self._h, rnd, ctypes.byref(v)))
+        return v.value
+
+    def amplitude_sum(self):
+        re, im = ctypes.c_double(), ctypes.c_double()
+        _check(lib().tmfqs_gpu_amplitude_sum(self._h, ctypes.byref(re), ctypes.byref(im)))
+        return re.value, im.value
+
+    def overlay_sum(self, scale, bias):
+        re, im = ctypes.c_double(), ctypes.c_double()
+        _check(lib().tmfqs_gpu_overlay_sum(self._h, scale[0], scale[1], bias[0], bias[1], ctypes.byref(re), ctypes.byref(im)))
+        return re.value, im.value
+
+    def overlay_total_probability(self, scale, bias) -> float:
+        v = ctypes.c_double()
+        _check(lib().tmfqs_gpu_overlay_total_probability(self._h, scale[0], scale[1], bias[0], bias[1], ctypes.byref(v)))
+        return v.value
+
+    def overlay_sample(self, scale, bias, rnd) -> int:
+        v = ctypes.c_uint64()
+        _check(lib().tmfqs_gpu_overlay_sample(self._h, scale[0], scale[1], bias[0], bias[1], rnd, ctypes.byref(v)))
+        return v.value
+
+    # -- operations --
+    def h(self, q):
+        _check(lib().tmfqs_gpu_h(self._h, q))
+
+    def x(self, q):
+        _check(lib().tmfqs_gpu_x(self._h, q))
+
+    def cnot(self, c, t):
+        _check(lib().tmfqs_gpu_cnot(self._h, c, t))
+
+    def cphase(self, c, t, theta):
+        _check(lib().tmfqs_gpu_cphase(self._h, c, t, theta))
+
+    def swap(self, a, b):
+        _check(lib().tmfqs_gpu_swap(self._h, a, b))
+
+    def gate(self, matrix: np.ndarray, qubits):
+        op = gate(matrix, qubits)
+        _check(lib().tmfqs_gpu_gate(self._h, op.matrix, op.qubits, op.k))
+
+    def phase_flip(self, s):
+        _check(lib().tmfqs_gpu_phase_flip(self._h, s))
+
+    def inversion(self):
+        _check(lib().tmfqs_gpu_inversion(self._h))
+
+    def inversion_mean(self, re, im):
+        _check(lib().tmfqs_gpu_inversion_mean(self._h, re, im))
+
+    def affine(self, scale, bias):
+        _check(lib().tmfqs_gpu_affine(self._h, scale[0], scale[1], bias[0], bias[1]))
+
+    def apply_ops(self, ops):
+        arr = op_array(ops)
+        _check(lib().tmfqs_gpu_apply_ops(self._h, arr, len(ops)))
+
+    def grover_run(self, view: RegisterView, marked, iterations: int, materialized: bool) -> RegisterView:
+        a = np.ascontiguousarray(np.array(marked, dtype=np.uint64))
+        _check(lib().tmfqs_gpu_grover_run(self._h, ctypes.byref(view), a.ctypes.data_as(_U64P), len(a), iterations,
+                                          1 if materialized else 0))
+        return view
+
+    def sync(self):
+        _check(lib().tmfqs_gpu_sync(self._h))
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(lib().tmfqs_gpu_stats(self._h, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def reset_stats(self):
+        _check(lib().tmfqs_gpu_reset_stats(self._h))
+
+    def set_option(self, option: int, value: int):
+        _check(lib().tmfqs_gpu_set_option(self._h, option, value))
+
+    def kernel_times(self) -> dict:
+        arr = (KernelTime * len(KT_NAMES))()
+        _check(lib().tmfqs_gpu_kernel_times(self._h, arr))
+        return {n: {"launches": arr[i].launches, "ms": arr[i].ms, "bytes": arr[i].bytes} for i, n in enumerate(KT_NAMES)}
+
+    def device_buffer(self):
+        p, n = ctypes.c_void_p(), ctypes.c_size_t()
+        _check(lib().tmfqs_gpu_device_buffer(self._h, ctypes.byref(p), ctypes.byref(n)))
+        return p.value, n.value
+
+    def stream(self):
+        p = ctypes.c_void_p()
+        _check(lib().tmfqs_gpu_stream(self._h, ctypes.byref(p)))
+        return p.value

@@ -1,0 +1,1271 @@
+// C ABI of libtmfqs_b200 (declared in include/tmfqs_b200.h).
+//
+// Validation mirrors the reference backend and register contracts
+// (core/validation.h:19-80, storage/common/backend_validation.h:13-39,
+// dense_state_backend.cpp:31-50) with 64-bit state counts.  Errors become
+// status codes plus a thread-local message.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "device_common.cuh"
+#include "internal.h"
+
+namespace tqb {
+
+void fail(int status, const std::string &message) { throw Error{status, message}; }
+
+void check_cuda(cudaError_t e, const char *what) {
+	if(e != cudaSuccess) {
+		cudaGetLastError();
+		throw Error{TMFQS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+	}
+}
+
+}  // namespace tqb
+
+namespace {
+
+using tqb::fail;
+using tqb::check_cuda;
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(F &&fn) {
+	try {
+		fn();
+		return TMFQS_OK;
+	} catch(const tqb::Error &e) {
+		g_last_error = e.message;
+		return e.status;
+	} catch(const std::bad_alloc &) {
+		g_last_error = "host allocation failed";
+		return TMFQS_ERR_NOMEM;
+	} catch(const std::exception &e) {
+		g_last_error = e.what();
+		return TMFQS_ERR_RUNTIME;
+	}
+}
+
+constexpr unsigned kMaxQubits = 40;
+constexpr size_t kPinnedElems = 3 * 4096;  // idx + 2 doubles per flushed entry
+
+struct DeviceScope {
+	explicit DeviceScope(const tmfqs_gpu_state *h) { check_cuda(cudaSetDevice(h->device), "cudaSetDevice"); }
+};
+
+tqb::LaunchCtx ctx(tmfqs_gpu_state *h) { return tqb::LaunchCtx{h->stream, h->num_sms, &h->stats.kernel_launches}; }
+
+size_t amp_bytes(const tmfqs_gpu_state *h) { return h->precision == TMFQS_FP64 ? 16 : 8; }
+
+// Records CUDA events around one pass when kernel timing is on.
+class PassTimer {
+	public:
+		PassTimer(tmfqs_gpu_state *h, int kind, double bytes) : h_(h), kind_(kind), bytes_(bytes) {
+			if(!h_->opt_timing) return;
+			check_cuda(cudaEventCreate(&start_), "timer event");
+			check_cuda(cudaEventCreate(&stop_), "timer event");
+			check_cuda(cudaEventRecord(start_, h_->stream), "timer record");
+		}
+		~PassTimer() {
+			if(!h_->opt_timing || !start_) return;
+			if(cudaEventRecord(stop_, h_->stream) == cudaSuccess) {
+				h_->timed.push_back({kind_, start_, stop_, bytes_});
+			} else {
+				cudaGetLastError();
+				cudaEventDestroy(start_);
+				cudaEventDestroy(stop_);
+			}
+		}
+	private:
+		tmfqs_gpu_state *h_;
+		int kind_;
+		double bytes_;
+		cudaEvent_t start_ = nullptr, stop_ = nullptr;
+};
+
+double sweep_bytes(const tmfqs_gpu_state *h) { return 2.0 * (double)h->N * (double)amp_bytes(h); }
+
+void resolve_timers(tmfqs_gpu_state *h) {
+	for(auto &t : h->timed) {
+		check_cuda(cudaEventSynchronize(t.stop), "timer sync");
+		float ms = 0.f;
+		check_cuda(cudaEventElapsedTime(&ms, t.start, t.stop), "timer elapsed");
+		h->times[t.kind].launches += 1;
+		h->times[t.kind].ms += ms;
+		h->times[t.kind].bytes += t.bytes;
+		cudaEventDestroy(t.start);
+		cudaEventDestroy(t.stop);
+	}
+	h->timed.clear();
+}
+
+void require_handle(tmfqs_gpu_state *h) {
+	if(!h) fail(TMFQS_ERR_INVALID_ARGUMENT, "null handle");
+}
+
+void ensure_initialized(tmfqs_gpu_state *h, const char *operation) {
+	require_handle(h);
+	if(!h->initialized) fail(TMFQS_ERR_LOGIC, std::string("GpuStateBackend is not initialized for ") + operation);
+}
+
+void validate_state(tmfqs_gpu_state *h, uint64_t s, const char *scope) {
+	if(s >= h->N) fail(TMFQS_ERR_OUT_OF_RANGE, std::string(scope) + " state index out of range");
+}
+
+void validate_qubit(tmfqs_gpu_state *h, unsigned q, const char *scope) {
+	if(q >= h->n) fail(TMFQS_ERR_OUT_OF_RANGE, std::string(scope) + " qubit index out of range");
+}
+
+void validate_two(tmfqs_gpu_state *h, unsigned a, unsigned b, const char *scope) {
+	validate_qubit(h, a, scope);
+	validate_qubit(h, b, scope);
+	if(a == b) fail(TMFQS_ERR_INVALID_ARGUMENT, std::string(scope) + " requires distinct qubits");
+}
+
+unsigned bit_of(const tmfqs_gpu_state *h, unsigned q) { return h->n - q - 1u; }
+
+// Allocates (or reuses) the device state for n qubits.
+void ensure_state(tmfqs_gpu_state *h, unsigned n) {
+	if(n > kMaxQubits) fail(TMFQS_ERR_INVALID_ARGUMENT, "Number of qubits exceeds supported range for this device build");
+	const size_t bytes = amp_bytes(h) << n;
+	if(h->amps && h->bytes == bytes) {
+		h->n = n;
+		h->N = 1ull << n;
+		return;
+	}
+	if(h->amps) {
+		check_cuda(cudaStreamSynchronize(h->stream), "sync before free");
+		cudaFree(h->amps);
+		h->amps = nullptr;
+		h->bytes = 0;
+	}
+	tqb::seq_scratch_free(h->seq);
+	if(cudaMalloc(&h->amps, bytes) != cudaSuccess) {
+		cudaGetLastError();
+		h->amps = nullptr;
+		h->initialized = false;
+		fail(TMFQS_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes for the state failed");
+	}
+	h->bytes = bytes;
+	h->n = n;
+	h->N = 1ull << n;
+}
+
+void ensure_dev_small(tmfqs_gpu_state *h, size_t bytes) {
+	if(h->dev_small_bytes >= bytes) return;
+	if(h->dev_small) {
+		check_cuda(cudaStreamSynchronize(h->stream), "sync before staging free");
+		cudaFree(h->dev_small);
+	}
+	h->dev_small = nullptr;
+	h->dev_small_bytes = 0;
+	const size_t sz = std::max<size_t>(bytes, 1 << 16);
+	if(cudaMalloc(&h->dev_small, sz) != cudaSuccess) {
+		cudaGetLastError();
+		fail(TMFQS_ERR_NOMEM, "device staging allocation failed");
+	}
+	h->dev_small_bytes = sz;
+}
+
+// Writes dirty cached amplitudes to the device (one scatter per 4096).
+void flush_dirty(tmfqs_gpu_state *h) {
+	if(h->dirty.empty()) return;
+	std::vector<uint64_t> idx;
+	idx.reserve(h->dirty.size());
+	for(const auto &kv : h->dirty) idx.push_back(kv.first);
+	std::sort(idx.begin(), idx.end());
+	ensure_dev_small(h, 4096 * 24);
+	for(size_t off = 0; off < idx.size(); off += 4096) {
+		const size_t cnt = std::min<size_t>(4096, idx.size() - off);
+		check_cuda(cudaStreamSynchronize(h->stream), "flush sync");
+		uint64_t *pi = reinterpret_cast<uint64_t *>(h->pinned);
+		double *pv = h->pinned + cnt;
+		for(size_t i = 0; i < cnt; ++i) {
+			pi[i] = idx[off + i];
+			const auto &v = h->cache[idx[off + i]];
+			pv[2 * i] = v.first;
+			pv[2 * i + 1] = v.second;
+		}
+		check_cuda(cudaMemcpyAsync(h->dev_small, h->pinned, cnt * 24, cudaMemcpyHostToDevice, h->stream), "flush upload");
+		const uint64_t *di = static_cast<const uint64_t *>(h->dev_small);
+		const double *dv = reinterpret_cast<const double *>(static_cast<unsigned char *>(h->dev_small) + cnt * 8);
+		tqb::launch_scatter_values(ctx(h), h->precision, h->amps, di, dv, cnt);
+		h->stats.h2d_bytes += cnt * 24;
+	}
+	h->dirty.clear();
+}
+
+// Before a kernel that mutates the state: push pending writes, drop the cache.
+void before_mutation(tmfqs_gpu_state *h) {
+	flush_dirty(h);
+	h->cache.clear();
+}
+
+// Round a value to the storage precision (what the device will hold).
+double to_storage(const tmfqs_gpu_state *h, double v) {
+	return h->precision == TMFQS_FP64 ? v : (double)(float)v;
+}
+
+std::pair<double, double> read_amp(tmfqs_gpu_state *h, uint64_t s) {
+	auto it = h->cache.find(s);
+	if(it != h->cache.end()) return it->second;
+	const size_t ab = amp_bytes(h);
+	check_cuda(cudaMemcpyAsync(h->pinned, static_cast<unsigned char *>(h->amps) + s * ab, ab, cudaMemcpyDeviceToHost,
+	                           h->stream),
+	           "amplitude read");
+	check_cuda(cudaStreamSynchronize(h->stream), "amplitude read sync");
+	h->stats.d2h_bytes += ab;
+	std::pair<double, double> v;
+	if(h->precision == TMFQS_FP64) {
+		v = {h->pinned[0], h->pinned[1]};
+	} else {
+		const float *f = reinterpret_cast<const float *>(h->pinned);
+		v = {(double)f[0], (double)f[1]};
+	}
+	h->cache[s] = v;
+	return v;
+}
+
+void write_amp(tmfqs_gpu_state *h, uint64_t s, double re, double im) {
+	h->cache[s] = {to_storage(h, re), to_storage(h, im)};
+	h->dirty[s] = true;
+}
+
+// Host <-> device copies of interleaved complex128 data, converting for
+// complex64 states through a device staging buffer.
+void copy_in(tmfqs_gpu_state *h, uint64_t first, const double *host, uint64_t count) {
+	if(count == 0) return;
+	if(h->precision == TMFQS_FP64) {
+		check_cuda(cudaMemcpyAsync(static_cast<double2 *>(h->amps) + first, host, count * 16, cudaMemcpyHostToDevice, h->stream), "load");
+	} else {
+		const uint64_t chunk = 1ull << 22;
+		ensure_dev_small(h, chunk * 16);
+		for(uint64_t off = 0; off < count; off += chunk) {
+			const uint64_t c = std::min<uint64_t>(chunk, count - off);
+			check_cuda(cudaMemcpyAsync(h->dev_small, host + 2 * off, c * 16, cudaMemcpyHostToDevice, h->stream), "load");
+			tqb::launch_to_c64(ctx(h), static_cast<float2 *>(h->amps) + first + off, static_cast<const double *>(h->dev_small), c);
+		}
+	}
+	h->stats.h2d_bytes += count * 16;
+}
+
+void copy_out(tmfqs_gpu_state *h, uint64_t first, double *host, uint64_t count) {
+	if(count == 0) return;
+	if(h->precision == TMFQS_FP64) {
+		check_cuda(cudaMemcpyAsync(host, static_cast<double2 *>(h->amps) + first, count * 16, cudaMemcpyDeviceToHost, h->stream), "export");
+	} else {
+		const uint64_t chunk = 1ull << 22;
+		ensure_dev_small(h, chunk * 16);
+		for(uint64_t off = 0; off < count; off += chunk) {
+			const uint64_t c = std::min<uint64_t>(chunk, count - off);
+			tqb::launch_from_c64(ctx(h), static_cast<double *>(h->dev_small), static_cast<const float2 *>(h->amps) + first + off, c);
+			check_cuda(cudaMemcpyAsync(host + 2 * off, h->dev_small, c * 16, cudaMemcpyDeviceToHost, h->stream), "export");
+		}
+	}
+	check_cuda(cudaStreamSynchronize(h->stream), "export sync");
+	h->stats.d2h_bytes += count * 16;
+}
+
+tqb::SeqResult reduce(tmfqs_gpu_state *h, tqb::TermKind kind, const tqb::Overlay &ov, bool stop, double rnd) {
+	flush_dirty(h);
+	h->stats.reduction_passes += 2;
+	PassTimer timer(h, TMFQS_KT_REDUCE, sweep_bytes(h));  // two read passes = one sweep's bytes
+	return tqb::seq_replay(h->precision, h->amps, h->N, kind, ov, stop, rnd, h->seq, h->stream, h->num_sms,
+	                       &h->stats.kernel_launches);
+}
+
+// ---------------------------------------------------------------------------
+// Fusion planner for tmfqs_gpu_apply_ops (the Simulator's gate runs).
+// ---------------------------------------------------------------------------
+struct Planner {
+	tmfqs_gpu_state *h;
+	unsigned K;     // local bits of a pass
+	unsigned mlow;  // low bits always local (row of >= 128 bytes)
+	tqb::FusedPass pass;
+	uint64_t tmask = 0;  // bits that must be local (moving bits of ops in the pass)
+	int chain_op = -1;   // index of the H-chain op that may still grow
+	unsigned chain_low = 64;  // lowest bit position in that chain so far
+	size_t nontrivial = 0;
+	std::vector<const tmfqs_op *> pending;  // circuit ops in the pass (for single-op fallback)
+
+	explicit Planner(tmfqs_gpu_state *hh) : h(hh) {
+		const unsigned Kmax = 12;  // 2^12 amplitudes: 64 KB (complex128) / 32 KB (complex64)
+		const unsigned q = h->opt_fused_qubits > 0 ? (unsigned)h->opt_fused_qubits : 9u;
+		mlow = h->precision == TMFQS_FP64 ? 3u : 4u;
+		K = std::min<unsigned>(h->n, std::min<unsigned>(Kmax + (h->precision == TMFQS_FP64 ? 0u : 1u), q + mlow));
+		reset();
+	}
+
+	void reset() {
+		pass = tqb::FusedPass{};
+		pass.n = h->n;
+		tmask = 0;
+		chain_op = -1;
+		chain_low = 64;
+		nontrivial = 0;
+		pending.clear();
+	}
+
+	// Whether bits in `m` can be local together with the current ones.
+	bool fits(uint64_t m) const {
+		const uint64_t all = tmask | m;
+		const uint64_t low = mlow >= 64 ? ~0ull : ((1ull << mlow) - 1ull);
+		const unsigned extra = (unsigned)__builtin_popcountll(all & ~low);
+		return extra + std::min(mlow, h->n) <= K;
+	}
+
+	unsigned local_index(unsigned bit) const {
+		for(unsigned i = 0; i < pass.K; ++i)
+			if(pass.lpos[i] == bit) return i;
+		fail(TMFQS_ERR_LOGIC, "planner: bit not local");
+	}
+
+	void finalize_local_set() {
+		std::vector<unsigned> L;
+		for(unsigned b = 0; b < h->n; ++b)
+			if((tmask >> b) & 1ull) L.push_back(b);
+		for(unsigned b = 0; b < h->n && L.size() < K; ++b)
+			if(!((tmask >> b) & 1ull)) L.push_back(b);
+		std::sort(L.begin(), L.end());
+		pass.K = (unsigned)L.size();
+		for(unsigned i = 0; i < pass.K; ++i) pass.lpos[i] = L[i];
+	}
+
+	// Ops are recorded with global bit positions in `lt`/`lc` and converted to
+	// local indices once the local set is known.
+	void flush() {
+		if(pending.empty()) return;
+		if(pending.size() == 1) {
+			run_single(*pending[0]);
+		} else {
+			finalize_local_set();
+			for(auto &op : pass.ops) {
+				if(op.kind == tqb::kFH || op.kind == tqb::kFHChain || op.kind == tqb::kFX || op.kind == tqb::kFCnot)
+					op.lt = local_index(op.lt);
+				if(op.kind == tqb::kFSwap) {
+					op.lt = local_index(op.lt);
+					op.lc = local_index(op.lc);
+				}
+			}
+			pass.gate_count = (unsigned)pending.size();
+			PassTimer timer(h, TMFQS_KT_FUSED, sweep_bytes(h));
+			tqb::launch_fused_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes);
+			++h->stats.fused_passes;
+		}
+		reset();
+	}
+
+	void run_single(const tmfqs_op &op) {
+		const auto c = ctx(h);
+		PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+		switch(op.kind) {
+			case TMFQS_OP_H: tqb::launch_h(c, h->precision, h->amps, h->n, bit_of(h, op.q0)); break;
+			case TMFQS_OP_X: tqb::launch_x(c, h->precision, h->amps, h->n, bit_of(h, op.q0)); break;
+			case TMFQS_OP_CNOT: tqb::launch_cnot(c, h->precision, h->amps, h->n, bit_of(h, op.q0), bit_of(h, op.q1)); break;
+			case TMFQS_OP_CPHASE:
+				tqb::launch_cphase(c, h->precision, h->amps, h->n, bit_of(h, op.q0), bit_of(h, op.q1), std::cos(op.theta), std::sin(op.theta));
+				break;
+			case TMFQS_OP_SWAP: tqb::launch_swap(c, h->precision, h->amps, h->n, bit_of(h, op.q0), bit_of(h, op.q1)); break;
+			case TMFQS_OP_PHASE_FLIP: tqb::launch_phase_flip(c, h->precision, h->amps, op.state); break;
+			default: fail(TMFQS_ERR_LOGIC, "planner: unexpected single op");
+		}
+		++h->stats.gate_passes;
+	}
+
+	void add_pair_op(const tmfqs_op &op, uint32_t kind, unsigned bit, uint64_t cmask) {
+		const uint64_t m = 1ull << bit;
+		if(!fits(m)) flush();
+		tmask |= m;
+		tqb::FusedOp f{};
+		f.kind = kind;
+		f.lt = bit;
+		f.mask = cmask;
+		pass.ops.push_back(f);
+		pending.push_back(&op);
+		++nontrivial;
+		chain_op = -1;
+		if(kind == tqb::kFH) {
+			// A Hadamard may grow into an H-chain with the phases that follow.
+			chain_op = (int)pass.ops.size() - 1;
+			chain_low = bit;
+		}
+	}
+
+	void add(const tmfqs_op &op) {
+		switch(op.kind) {
+			case TMFQS_OP_H: add_pair_op(op, tqb::kFH, bit_of(h, op.q0), 0); return;
+			case TMFQS_OP_X: add_pair_op(op, tqb::kFX, bit_of(h, op.q0), 0); return;
+			case TMFQS_OP_CNOT: add_pair_op(op, tqb::kFCnot, bit_of(h, op.q1), 1ull << bit_of(h, op.q0)); return;
+			case TMFQS_OP_SWAP: {
+				const unsigned a = bit_of(h, op.q0), b = bit_of(h, op.q1);
+				const uint64_t m = (1ull << a) | (1ull << b);
+				if(!fits(m)) flush();
+				tmask |= m;
+				tqb::FusedOp f{};
+				f.kind = tqb::kFSwap;
+				f.lt = a;
+				f.lc = b;
+				pass.ops.push_back(f);
+				pending.push_back(&op);
+				chain_op = -1;
+				return;
+			}
+			case TMFQS_OP_CPHASE: {
+				const unsigned bc = bit_of(h, op.q0), bt = bit_of(h, op.q1);
+				const double cr = std::cos(op.theta), ci = std::sin(op.theta);  // dense_state_backend.cpp:293-294
+				if(chain_op >= 0) {
+					tqb::FusedOp &ch = pass.ops[chain_op];
+					const unsigned hb = ch.lt;  // global bit of the chain's Hadamard
+					const int other = bc == hb ? (int)bt : (bt == hb ? (int)bc : -1);
+					if(other >= 0 && (unsigned)other < chain_low) {
+						if(ch.kind == tqb::kFH) {
+							ch.kind = tqb::kFHChain;
+							ch.tab = (uint32_t)(pass.phases.size() / 2);
+							pass.phases.resize(pass.phases.size() + 128, 0.0);
+						}
+						ch.mask |= 1ull << other;
+						pass.phases[2 * (ch.tab + other)] = cr;
+						pass.phases[2 * (ch.tab + other) + 1] = ci;
+						chain_low = (unsigned)other;
+						pending.push_back(&op);
+						return;
+					}
+				}
+				tqb::FusedOp f{};
+				f.kind = tqb::kFCP;
+				f.mask = (1ull << bc) | (1ull << bt);
+				f.cr = cr;
+				f.ci = ci;
+				pass.ops.push_back(f);
+				pending.push_back(&op);
+				chain_op = -1;
+				return;
+			}
+			case TMFQS_OP_PHASE_FLIP: {
+				tqb::FusedOp f{};
+				f.kind = tqb::kFFlip;
+				f.state = op.state;
+				pass.ops.push_back(f);
+				pending.push_back(&op);
+				chain_op = -1;
+				return;
+			}
+			default: fail(TMFQS_ERR_LOGIC, "planner: unsupported op in fused pass");
+		}
+	}
+};
+
+// Validates one op in the register's order of checks (QuantumRegister
+// methods, quantum_register.cpp:394-527; validateGateTargets,
+// validation.h:53-80).
+void validate_op(tmfqs_gpu_state *h, const tmfqs_op &op) {
+	switch(op.kind) {
+		case TMFQS_OP_H: validate_qubit(h, op.q0, "QuantumRegister::applyHadamard"); return;
+		case TMFQS_OP_X: validate_qubit(h, op.q0, "QuantumRegister::applyPauliX"); return;
+		case TMFQS_OP_CNOT: validate_two(h, op.q0, op.q1, "QuantumRegister::applyControlledNot"); return;
+		case TMFQS_OP_CPHASE: validate_two(h, op.q0, op.q1, "QuantumRegister::applyControlledPhaseShift"); return;
+		case TMFQS_OP_SWAP: validate_two(h, op.q0, op.q1, "QuantumRegister::applySwap"); return;
+		case TMFQS_OP_PHASE_FLIP: validate_state(h, op.state, "QuantumRegister::applyPhaseFlipBasisState"); return;
+		case TMFQS_OP_GATE: {
+			if(op.k > h->n) fail(TMFQS_ERR_INVALID_ARGUMENT, "QuantumRegister::applyGate gate acts on more qubits than available");
+			if(!op.matrix || (op.k && !op.qubits)) fail(TMFQS_ERR_INVALID_ARGUMENT, "QuantumRegister::applyGate null matrix or qubits");
+			std::vector<bool> seen(h->n, false);
+			for(unsigned i = 0; i < op.k; ++i) {
+				validate_qubit(h, op.qubits[i], "QuantumRegister::applyGate");
+				if(seen[op.qubits[i]]) fail(TMFQS_ERR_INVALID_ARGUMENT, "QuantumRegister::applyGate duplicate qubit index");
+				seen[op.qubits[i]] = true;
+			}
+			if(op.k > 10) fail(TMFQS_ERR_INVALID_ARGUMENT, "applyGate: this device build applies gates on at most 10 qubits");
+			return;
+		}
+		case TMFQS_OP_INVERSION:
+			fail(TMFQS_ERR_INVALID_ARGUMENT, "apply_ops: inversion about the mean needs register state; use tmfqs_gpu_grover_run");
+		default: fail(TMFQS_ERR_INVALID_ARGUMENT, "apply_ops: unknown operation kind");
+	}
+}
+
+void run_gate(tmfqs_gpu_state *h, const double *matrix, const unsigned *qubits, unsigned k) {
+	const size_t dim = 1ull << k;
+	const size_t mbytes = dim * dim * 16;
+	ensure_dev_small(h, mbytes);
+	check_cuda(cudaStreamSynchronize(h->stream), "gate staging sync");
+	check_cuda(cudaMemcpyAsync(h->dev_small, matrix, mbytes, cudaMemcpyHostToDevice, h->stream), "gate matrix upload");
+	std::vector<unsigned> tpos(k);
+	for(unsigned i = 0; i < k; ++i) tpos[i] = bit_of(h, qubits[i]);
+	{
+		PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+		tqb::launch_gate(ctx(h), h->precision, h->amps, h->n, k, static_cast<const double *>(h->dev_small), tpos.data());
+	}
+	check_cuda(cudaStreamSynchronize(h->stream), "gate sync");
+	++h->stats.gate_passes;
+}
+
+// A maximal run of >= 2 swaps on pairwise-disjoint qubits starting at i.
+size_t swap_run(const tmfqs_op *ops, size_t i, size_t count) {
+	uint64_t used = 0;
+	size_t j = i;
+	while(j < count && ops[j].kind == TMFQS_OP_SWAP && ops[j].q0 != ops[j].q1 && ops[j].q0 < 64 && ops[j].q1 < 64) {
+		const uint64_t m = (1ull << ops[j].q0) | (1ull << ops[j].q1);
+		if(used & m) break;
+		used |= m;
+		++j;
+	}
+	return j - i;
+}
+
+// ---- QuantumRegister arithmetic on the host (quantum_register.cpp:21-57) ----
+struct Cx {
+	double re, im;
+};
+Cx cadd(Cx a, Cx b) { return {a.re + b.re, a.im + b.im}; }
+Cx csub(Cx a, Cx b) { return {a.re - b.re, a.im - b.im}; }
+Cx cneg(Cx a) { return {-a.re, -a.im}; }
+Cx cscale(Cx a, double s) { return {a.re * s, a.im * s}; }
+Cx cmul(Cx l, Cx r) { return {l.re * r.re - l.im * r.im, l.re * r.im + l.im * r.re}; }
+Cx cdiv(Cx n, Cx d) {
+	const double q = d.re * d.re + d.im * d.im;
+	if(q == 0.0) fail(TMFQS_ERR_LOGIC, "QuantumRegister affine overlay scale is zero");
+	return {(n.re * d.re + n.im * d.im) / q, (n.im * d.re - n.re * d.im) / q};
+}
+
+Cx overlay_apply(const tmfqs_register_view &v, Cx a) {
+	if(!v.overlay) return a;
+	return cadd(cmul({v.scale_re, v.scale_im}, a), {v.bias_re, v.bias_im});
+}
+Cx overlay_remove(const tmfqs_register_view &v, Cx l) {
+	if(!v.overlay) return l;
+	return cdiv(csub(l, {v.bias_re, v.bias_im}), {v.scale_re, v.scale_im});
+}
+
+// Exact logical amplitude sum (quantum_register.cpp:176-190).
+Cx logical_sum(tmfqs_gpu_state *h, const tmfqs_register_view &v) {
+	tqb::Overlay ov;
+	ov.active = v.overlay != 0;
+	ov.sre = v.scale_re;
+	ov.sim = v.scale_im;
+	ov.bre = v.bias_re;
+	ov.bim = v.bias_im;
+	const double re = reduce(h, tqb::kTermReal, ov, false, 0.0).value;
+	const double im = reduce(h, tqb::kTermImag, ov, false, 0.0).value;
+	return {re, im};
+}
+
+// Device value a float-stored state holds after `tr - v` in float.
+template <typename S>
+S storage_sub(double t, S v) {
+	return (S)t - v;
+}
+
+template <typename S>
+void grover_materialized_fused(tmfqs_gpu_state *h, tmfqs_register_view *view, const std::vector<uint64_t> &marked,
+                               uint64_t iters) {
+	const double N = (double)h->N;
+	uint64_t flip_from = 0;
+	if(!view->has_sum) {
+		// Iteration 0: flips without reads (no cached sum, no overlay), then
+		// the exact logical sum of the flipped state.
+		before_mutation(h);
+		for(uint64_t s : marked) tqb::launch_phase_flip(ctx(h), h->precision, h->amps, s);
+		const Cx sum = logical_sum(h, *view);
+		view->has_sum = 1;
+		view->sum_re = sum.re;
+		view->sum_im = sum.im;
+		flip_from = 1;
+	}
+	std::vector<S> vr(marked.size()), vi(marked.size());
+	for(size_t q = 0; q < marked.size(); ++q) {
+		const auto a = read_amp(h, marked[q]);
+		vr[q] = (S)a.first;
+		vi[q] = (S)a.second;
+	}
+	std::vector<double> tm(2 * iters);
+	double sr = view->sum_re, si = view->sum_im;
+	for(uint64_t k = 0; k < iters; ++k) {
+		if(k >= flip_from) {
+			for(size_t q = 0; q < marked.size(); ++q) {
+				// applyPhaseFlipBasisState with a cached sum, no overlay (:408-419).
+				sr -= 2.0 * (double)vr[q];
+				si -= 2.0 * (double)vi[q];
+				vr[q] = -vr[q];
+				vi[q] = -vi[q];
+			}
+		}
+		// applyInversionAboutMeanMaterialized() (:447-467).
+		const double mr = sr / N, mi = si / N;
+		sr = 2.0 * mr * N - sr;
+		si = 2.0 * mi * N - si;
+		tm[2 * k] = 2.0 * mr;
+		tm[2 * k + 1] = 2.0 * mi;
+		for(size_t q = 0; q < marked.size(); ++q) {
+			vr[q] = storage_sub<S>(tm[2 * k], vr[q]);
+			vi[q] = storage_sub<S>(tm[2 * k + 1], vi[q]);
+		}
+	}
+	before_mutation(h);
+	const size_t tm_bytes = iters * 16, mk_bytes = marked.size() * 8;
+	const size_t off = (tm_bytes + 255) & ~size_t(255);
+	ensure_dev_small(h, off + mk_bytes);
+	check_cuda(cudaStreamSynchronize(h->stream), "grover staging sync");
+	check_cuda(cudaMemcpyAsync(h->dev_small, tm.data(), tm_bytes, cudaMemcpyHostToDevice, h->stream), "grover means upload");
+	check_cuda(cudaMemcpyAsync(static_cast<unsigned char *>(h->dev_small) + off, marked.data(), mk_bytes, cudaMemcpyHostToDevice, h->stream), "grover marked upload");
+	PassTimer timer(h, TMFQS_KT_GROVER, sweep_bytes(h));
+	tqb::launch_grover_temporal(ctx(h), h->precision, h->amps, h->n, static_cast<const double *>(h->dev_small), iters,
+	                            reinterpret_cast<const uint64_t *>(static_cast<unsigned char *>(h->dev_small) + off),
+	                            (unsigned)marked.size(), flip_from);
+	check_cuda(cudaStreamSynchronize(h->stream), "grover sync");
+	++h->stats.fused_passes;
+	view->sum_re = sr;
+	view->sum_im = si;
+	for(size_t q = 0; q < marked.size(); ++q) h->cache[marked[q]] = {(double)vr[q], (double)vi[q]};
+}
+
+// One phase flip with register semantics (quantum_register.cpp:405-420).
+void register_flip(tmfqs_gpu_state *h, tmfqs_register_view *v, uint64_t s) {
+	if(v->has_sum || v->overlay) {
+		const auto b = read_amp(h, s);
+		const Cx logical = overlay_apply(*v, {b.first, b.second});
+		if(v->has_sum) {
+			v->sum_re -= 2.0 * logical.re;
+			v->sum_im -= 2.0 * logical.im;
+		}
+		if(v->overlay) {
+			const Cx nb = overlay_remove(*v, cneg(logical));
+			write_amp(h, s, nb.re, nb.im);
+			return;
+		}
+	}
+	auto it = h->cache.find(s);
+	if(it != h->cache.end()) {
+		write_amp(h, s, -it->second.first, -it->second.second);
+		return;
+	}
+	flush_dirty(h);
+	tqb::launch_phase_flip(ctx(h), h->precision, h->amps, s);
+}
+
+// applyInversionAboutMean[Materialized]() with register semantics (:423-467).
+void register_inversion(tmfqs_gpu_state *h, tmfqs_register_view *v, bool materialized) {
+	if(!v->has_sum) {
+		const Cx s = logical_sum(h, *v);
+		v->has_sum = 1;
+		v->sum_re = s.re;
+		v->sum_im = s.im;
+	}
+	const double N = (double)h->N;
+	const Cx mean{v->sum_re / N, v->sum_im / N};
+	v->sum_re = 2.0 * mean.re * N - v->sum_re;
+	v->sum_im = 2.0 * mean.im * N - v->sum_im;
+	if(materialized) {
+		if(v->overlay) {
+			before_mutation(h);
+			{
+				PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+				tqb::launch_affine(ctx(h), h->precision, h->amps, h->n, v->scale_re, v->scale_im, v->bias_re, v->bias_im);
+			}
+			v->overlay = 0;
+			v->scale_re = 1.0;
+			v->scale_im = 0.0;
+			v->bias_re = 0.0;
+			v->bias_im = 0.0;
+		}
+		before_mutation(h);
+		{
+			PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+			tqb::launch_inversion(ctx(h), h->precision, h->amps, h->n, 2.0 * mean.re, 2.0 * mean.im);
+		}
+		++h->stats.gate_passes;
+		return;
+	}
+	const Cx scale = v->overlay ? Cx{v->scale_re, v->scale_im} : Cx{1.0, 0.0};
+	const Cx bias = v->overlay ? Cx{v->bias_re, v->bias_im} : Cx{0.0, 0.0};
+	const Cx ns = cneg(scale);
+	const Cx nb = csub(cscale(mean, 2.0), bias);
+	v->scale_re = ns.re;
+	v->scale_im = ns.im;
+	v->bias_re = nb.re;
+	v->bias_im = nb.im;
+	v->overlay = 1;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Public entry points
+// ===========================================================================
+extern "C" {
+
+const char *tmfqs_gpu_last_error(void) { return g_last_error.c_str(); }
+
+int tmfqs_gpu_create(int precision, int device, tmfqs_gpu_state **out) {
+	return guarded([&] {
+		if(!out) fail(TMFQS_ERR_INVALID_ARGUMENT, "null output handle");
+		*out = nullptr;
+		if(precision != TMFQS_FP64 && precision != TMFQS_FP32) fail(TMFQS_ERR_INVALID_ARGUMENT, "unknown precision");
+		int count = 0;
+		const cudaError_t e = cudaGetDeviceCount(&count);
+		if(e != cudaSuccess || count == 0) {
+			cudaGetLastError();
+			fail(TMFQS_ERR_CUDA, "no CUDA device available for the gpu storage strategy");
+		}
+		if(device < 0 || device >= count) fail(TMFQS_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+		auto *h = new tmfqs_gpu_state();
+		h->device = device;
+		h->precision = precision;
+		try {
+			check_cuda(cudaSetDevice(device), "cudaSetDevice");
+			check_cuda(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+			check_cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream create");
+			if(cudaMallocHost(&h->pinned, kPinnedElems * sizeof(double)) != cudaSuccess) {
+				cudaGetLastError();
+				fail(TMFQS_ERR_NOMEM, "pinned staging allocation failed");
+			}
+			h->pinned_elems = kPinnedElems;
+		} catch(...) {
+			if(h->stream) cudaStreamDestroy(h->stream);
+			delete h;
+			throw;
+		}
+		*out = h;
+	});
+}
+
+int tmfqs_gpu_destroy(tmfqs_gpu_state *h) {
+	if(!h) return TMFQS_OK;
+	return guarded([&] {
+		cudaSetDevice(h->device);
+		if(h->stream) cudaStreamSynchronize(h->stream);
+		for(auto &t : h->timed) {
+			cudaEventDestroy(t.start);
+			cudaEventDestroy(t.stop);
+		}
+		tqb::seq_scratch_free(h->seq);
+		if(h->amps) cudaFree(h->amps);
+		if(h->dev_small) cudaFree(h->dev_small);
+		if(h->dev_prog) cudaFree(h->dev_prog);
+		if(h->pinned) cudaFreeHost(h->pinned);
+		if(h->stream) cudaStreamDestroy(h->stream);
+		delete h;
+	});
+}
+
+int tmfqs_gpu_clone(tmfqs_gpu_state *h, tmfqs_gpu_state **out) {
+	return guarded([&] {
+		require_handle(h);
+		if(!out) fail(TMFQS_ERR_INVALID_ARGUMENT, "null output handle");
+		tmfqs_gpu_state *c = nullptr;
+		const int rc = tmfqs_gpu_create(h->precision, h->device, &c);
+		if(rc) throw tqb::Error{rc, g_last_error};
+		try {
+			DeviceScope d(h);
+			c->opt_fusion = h->opt_fusion;
+			c->opt_fused_qubits = h->opt_fused_qubits;
+			c->opt_grover_fusion = h->opt_grover_fusion;
+			if(h->initialized) {
+				flush_dirty(h);
+				ensure_state(c, h->n);
+				check_cuda(cudaStreamSynchronize(h->stream), "clone sync");
+				check_cuda(cudaMemcpyAsync(c->amps, h->amps, h->bytes, cudaMemcpyDeviceToDevice, c->stream), "clone copy");
+				check_cuda(cudaStreamSynchronize(c->stream), "clone copy sync");
+				c->initialized = true;
+			}
+		} catch(...) {
+			tmfqs_gpu_destroy(c);
+			throw;
+		}
+		*out = c;
+	});
+}
+
+int tmfqs_gpu_init_zero(tmfqs_gpu_state *h, unsigned n) {
+	return guarded([&] {
+		require_handle(h);
+		DeviceScope d(h);
+		ensure_state(h, n);
+		h->cache.clear();
+		h->dirty.clear();
+		check_cuda(cudaMemsetAsync(h->amps, 0, h->bytes, h->stream), "init zero");
+		h->initialized = true;
+	});
+}
+
+int tmfqs_gpu_init_basis(tmfqs_gpu_state *h, unsigned n, uint64_t s, double re, double im) {
+	return guarded([&] {
+		require_handle(h);
+		if(n <= kMaxQubits && s >= (1ull << n)) fail(TMFQS_ERR_OUT_OF_RANGE, "GpuStateBackend::initBasis state index out of range");
+		DeviceScope d(h);
+		ensure_state(h, n);
+		h->cache.clear();
+		h->dirty.clear();
+		check_cuda(cudaMemsetAsync(h->amps, 0, h->bytes, h->stream), "init basis");
+		h->initialized = true;
+		write_amp(h, s, re, im);
+		flush_dirty(h);
+	});
+}
+
+int tmfqs_gpu_init_uniform(tmfqs_gpu_state *h, unsigned n, const uint64_t *states, size_t count) {
+	return guarded([&] {
+		require_handle(h);
+		if(n > kMaxQubits) fail(TMFQS_ERR_INVALID_ARGUMENT, "Number of qubits exceeds supported range for this device build");
+		if(count && !states) fail(TMFQS_ERR_INVALID_ARGUMENT, "null state list");
+		std::vector<uint64_t> sel(states, states + count);
+		for(uint64_t s : sel)
+			if(s >= (1ull << n)) fail(TMFQS_ERR_OUT_OF_RANGE, "GpuStateBackend::initUniformSuperposition state index out of range");
+		std::sort(sel.begin(), sel.end());
+		sel.erase(std::unique(sel.begin(), sel.end()), sel.end());
+		if(sel.empty()) fail(TMFQS_ERR_INVALID_ARGUMENT, "GpuStateBackend::initUniformSuperposition requires at least one state");
+		DeviceScope d(h);
+		ensure_state(h, n);
+		h->cache.clear();
+		h->dirty.clear();
+		check_cuda(cudaMemsetAsync(h->amps, 0, h->bytes, h->stream), "init uniform");
+		const double amp = 1.0 / std::sqrt(static_cast<double>(sel.size()));  // dense_state_backend.cpp:110
+		const uint64_t chunk = 1ull << 20;
+		ensure_dev_small(h, chunk * 8);
+		for(uint64_t off = 0; off < sel.size(); off += chunk) {
+			const uint64_t c = std::min<uint64_t>(chunk, sel.size() - off);
+			check_cuda(cudaStreamSynchronize(h->stream), "uniform staging sync");
+			check_cuda(cudaMemcpyAsync(h->dev_small, sel.data() + off, c * 8, cudaMemcpyHostToDevice, h->stream), "uniform upload");
+			tqb::launch_scatter_uniform(ctx(h), h->precision, h->amps, static_cast<const uint64_t *>(h->dev_small), c, amp);
+		}
+		check_cuda(cudaStreamSynchronize(h->stream), "uniform sync");
+		h->initialized = true;
+	});
+}
+
+int tmfqs_gpu_load(tmfqs_gpu_state *h, unsigned n, const double *host) {
+	return guarded([&] {
+		require_handle(h);
+		if(!host) fail(TMFQS_ERR_INVALID_ARGUMENT, "null amplitude buffer");
+		DeviceScope d(h);
+		ensure_state(h, n);
+		h->cache.clear();
+		h->dirty.clear();
+		copy_in(h, 0, host, h->N);
+		check_cuda(cudaStreamSynchronize(h->stream), "load sync");
+		h->initialized = true;
+	});
+}
+
+int tmfqs_gpu_load_chunk(tmfqs_gpu_state *h, uint64_t first, const double *host, uint64_t count) {
+	return guarded([&] {
+		ensure_initialized(h, "amplitude loading");
+		if(!host && count) fail(TMFQS_ERR_INVALID_ARGUMENT, "null amplitude buffer");
+		if(first > h->N || count > h->N - first) fail(TMFQS_ERR_OUT_OF_RANGE, "load_chunk range out of range");
+		DeviceScope d(h);
+		before_mutation(h);
+		copy_in(h, first, host, count);
+		check_cuda(cudaStreamSynchronize(h->stream), "load sync");
+	});
+}
+
+int tmfqs_gpu_export(tmfqs_gpu_state *h, double *out) {
+	return guarded([&] {
+		ensure_initialized(h, "amplitude export");
+		if(!out) fail(TMFQS_ERR_INVALID_ARGUMENT, "null output buffer");
+		DeviceScope d(h);
+		flush_dirty(h);
+		copy_out(h, 0, out, h->N);
+	});
+}
+
+int tmfqs_gpu_export_chunk(tmfqs_gpu_state *h, uint64_t first, double *out, uint64_t count) {
+	return guarded([&] {
+		ensure_initialized(h, "amplitude chunk iteration");
+		if(!out && count) fail(TMFQS_ERR_INVALID_ARGUMENT, "null output buffer");
+		if(first > h->N || count > h->N - first) fail(TMFQS_ERR_OUT_OF_RANGE, "export_chunk range out of range");
+		DeviceScope d(h);
+		flush_dirty(h);
+		copy_out(h, first, out, count);
+	});
+}
+
+int tmfqs_gpu_get_amp(tmfqs_gpu_state *h, uint64_t s, double *re, double *im) {
+	return guarded([&] {
+		ensure_initialized(h, "amplitude query");
+		validate_state(h, s, "GpuStateBackend::amplitude");
+		DeviceScope d(h);
+		const auto v = read_amp(h, s);
+		*re = v.first;
+		*im = v.second;
+	});
+}
+
+int tmfqs_gpu_set_amp(tmfqs_gpu_state *h, uint64_t s, double re, double im) {
+	return guarded([&] {
+		ensure_initialized(h, "state update");
+		validate_state(h, s, "GpuStateBackend::setAmplitude");
+		write_amp(h, s, re, im);
+	});
+}
+
+int tmfqs_gpu_num_qubits(tmfqs_gpu_state *h, unsigned *out) {
+	return guarded([&] {
+		require_handle(h);
+		*out = h->n;
+	});
+}
+
+int tmfqs_gpu_precision(tmfqs_gpu_state *h, int *out) {
+	return guarded([&] {
+		require_handle(h);
+		*out = h->precision;
+	});
+}
+
+int tmfqs_gpu_total_probability(tmfqs_gpu_state *h, double *out) {
+	return guarded([&] {
+		ensure_initialized(h, "total probability query");
+		DeviceScope d(h);
+		*out = reduce(h, tqb::kTermProb, tqb::Overlay{}, false, 0.0).value;
+	});
+}
+
+int tmfqs_gpu_sample(tmfqs_gpu_state *h, double rnd, uint64_t *out) {
+	return guarded([&] {
+		ensure_initialized(h, "measurement");
+		if(!(rnd >= 0.0 && rnd < 1.0)) fail(TMFQS_ERR_INVALID_ARGUMENT, "GpuStateBackend::sampleMeasurement requires rnd in [0,1)");
+		DeviceScope d(h);
+		const tqb::SeqResult r = reduce(h, tqb::kTermProb, tqb::Overlay{}, true, rnd);
+		if(r.index >= h->N) fail(TMFQS_ERR_RUNTIME, "GpuStateBackend::sampleMeasurement cumulative probability did not reach sample");
+		*out = r.index;
+	});
+}
+
+int tmfqs_gpu_amplitude_sum(tmfqs_gpu_state *h, double *re, double *im) {
+	return guarded([&] {
+		ensure_initialized(h, "amplitude sum");
+		DeviceScope d(h);
+		*re = reduce(h, tqb::kTermReal, tqb::Overlay{}, false, 0.0).value;
+		*im = reduce(h, tqb::kTermImag, tqb::Overlay{}, false, 0.0).value;
+	});
+}
+
+int tmfqs_gpu_overlay_sum(tmfqs_gpu_state *h, double sre, double sim, double bre, double bim, double *re, double *im) {
+	return guarded([&] {
+		ensure_initialized(h, "amplitude sum");
+		DeviceScope d(h);
+		const tqb::Overlay ov{true, sre, sim, bre, bim};
+		*re = reduce(h, tqb::kTermReal, ov, false, 0.0).value;
+		*im = reduce(h, tqb::kTermImag, ov, false, 0.0).value;
+	});
+}
+
+int tmfqs_gpu_overlay_total_probability(tmfqs_gpu_state *h, double sre, double sim, double bre, double bim, double *out) {
+	return guarded([&] {
+		ensure_initialized(h, "probability summation");
+		DeviceScope d(h);
+		*out = reduce(h, tqb::kTermProb, tqb::Overlay{true, sre, sim, bre, bim}, false, 0.0).value;
+	});
+}
+
+int tmfqs_gpu_overlay_sample(tmfqs_gpu_state *h, double sre, double sim, double bre, double bim, double rnd, uint64_t *out) {
+	return guarded([&] {
+		ensure_initialized(h, "measurement");
+		DeviceScope d(h);
+		const tqb::SeqResult r = reduce(h, tqb::kTermProb, tqb::Overlay{true, sre, sim, bre, bim}, true, rnd);
+		if(r.index >= h->N) fail(TMFQS_ERR_RUNTIME, "QuantumRegister::measure cumulative probability did not reach sample");
+		*out = r.index;
+	});
+}
+
+int tmfqs_gpu_phase_flip(tmfqs_gpu_state *h, uint64_t s) {
+	return guarded([&] {
+		ensure_initialized(h, "basis-state phase flip");
+		validate_state(h, s, "GpuStateBackend::phaseFlipBasisState");
+		DeviceScope d(h);
+		auto it = h->cache.find(s);
+		if(it != h->cache.end()) {
+			write_amp(h, s, -it->second.first, -it->second.second);
+			return;
+		}
+		flush_dirty(h);
+		tqb::launch_phase_flip(ctx(h), h->precision, h->amps, s);
+	});
+}
+
+int tmfqs_gpu_inversion_mean(tmfqs_gpu_state *h, double re, double im) {
+	return guarded([&] {
+		ensure_initialized(h, "inversion about mean");
+		DeviceScope d(h);
+		before_mutation(h);
+		{
+			PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+			tqb::launch_inversion(ctx(h), h->precision, h->amps, h->n, 2.0 * re, 2.0 * im);
+		}
+		++h->stats.gate_passes;
+	});
+}
+
+int tmfqs_gpu_inversion(tmfqs_gpu_state *h) {
+	return guarded([&] {
+		ensure_initialized(h, "inversion about mean");
+		DeviceScope d(h);
+		const double sr = reduce(h, tqb::kTermReal, tqb::Overlay{}, false, 0.0).value;
+		const double si = reduce(h, tqb::kTermImag, tqb::Overlay{}, false, 0.0).value;
+		const double N = (double)h->N;
+		before_mutation(h);
+		{
+			PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+			tqb::launch_inversion(ctx(h), h->precision, h->amps, h->n, 2.0 * (sr / N), 2.0 * (si / N));
+		}
+		++h->stats.gate_passes;
+	});
+}
+
+int tmfqs_gpu_affine(tmfqs_gpu_state *h, double sre, double sim, double bre, double bim) {
+	return guarded([&] {
+		ensure_initialized(h, "affine transform");
+		DeviceScope d(h);
+		before_mutation(h);
+		{
+			PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+			tqb::launch_affine(ctx(h), h->precision, h->amps, h->n, sre, sim, bre, bim);
+		}
+		++h->stats.gate_passes;
+	});
+}
+
+int tmfqs_gpu_h(tmfqs_gpu_state *h, unsigned q) {
+	return guarded([&] {
+		ensure_initialized(h, "DenseStateBackend::applyHadamard");
+		validate_qubit(h, q, "GpuStateBackend::applyHadamard");
+		DeviceScope d(h);
+		before_mutation(h);
+		{
+			PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+			tqb::launch_h(ctx(h), h->precision, h->amps, h->n, bit_of(h, q));
+		}
+		++h->stats.gate_passes;
+	});
+}
+
+int tmfqs_gpu_x(tmfqs_gpu_state *h, unsigned q) {
+	return guarded([&] {
+		ensure_initialized(h, "GpuStateBackend::applyPauliX");
+		validate_qubit(h, q, "GpuStateBackend::applyPauliX");
+		DeviceScope d(h);
+		before_mutation(h);
+		{
+			PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+			tqb::launch_x(ctx(h), h->precision, h->amps, h->n, bit_of(h, q));
+		}
+		++h->stats.gate_passes;
+	});
+}
+
+int tmfqs_gpu_cphase(tmfqs_gpu_state *h, unsigned c, unsigned t, double theta) {
+	return guarded([&] {
+		ensure_initialized(h, "GpuStateBackend::applyControlledPhaseShift");
+		validate_two(h, c, t, "GpuStateBackend::applyControlledPhaseShift");
+		DeviceScope d(h);
+		before_mutation(h);
+		{
+			PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+			tqb::launch_cphase(ctx(h), h->precision, h->amps, h->n, bit_of(h, c), bit_of(h, t), std::cos(theta), std::sin(theta));
+		}
+		++h->stats.gate_passes;
+	});
+}
+
+int tmfqs_gpu_cnot(tmfqs_gpu_state *h, unsigned c, unsigned t) {
+	return guarded([&] {
+		ensure_initialized(h, "GpuStateBackend::applyControlledNot");
+		validate_two(h, c, t, "GpuStateBackend::applyControlledNot");
+		DeviceScope d(h);
+		before_mutation(h);
+		{
+			PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+			tqb::launch_cnot(ctx(h), h->precision, h->amps, h->n, bit_of(h, c), bit_of(h, t));
+		}
+		++h->stats.gate_passes;
+	});
+}
+
+int tmfqs_gpu_swap(tmfqs_gpu_state *h, unsigned a, unsigned b) {
+	return guarded([&] {
+		ensure_initialized(h, "swap");
+		validate_two(h, a, b, "GpuStateBackend::applySwap");
+		DeviceScope d(h);
+		before_mutation(h);
+		{
+			PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+			tqb::launch_swap(ctx(h), h->precision, h->amps, h->n, bit_of(h, a), bit_of(h, b));
+		}
+		++h->stats.gate_passes;
+	});
+}
+
+int tmfqs_gpu_gate(tmfqs_gpu_state *h, const double *matrix, const unsigned *qubits, unsigned k) {
+	return guarded([&] {
+		ensure_initialized(h, "gate application");
+		tmfqs_op op{};
+		op.kind = TMFQS_OP_GATE;
+		op.matrix = matrix;
+		op.qubits = qubits;
+		op.k = k;
+		validate_op(h, op);
+		DeviceScope d(h);
+		before_mutation(h);
+		run_gate(h, matrix, qubits, k);
+	});
+}
+
+int tmfqs_gpu_apply_ops(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count) {
+	return guarded([&] {
+		ensure_initialized(h, "operation batch");
+		if(count && !ops) fail(TMFQS_ERR_INVALID_ARGUMENT, "null op list");
+		DeviceScope d(h);
+		before_mutation(h);
+		if(!h->opt_fusion) {
+			for(size_t i = 0; i < count; ++i) {
+				validate_op(h, ops[i]);
+				Planner p(h);
+				if(ops[i].kind == TMFQS_OP_GATE) run_gate(h, ops[i].matrix, ops[i].qubits, ops[i].k);
+				else p.run_single(ops[i]);
+			}
+			check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
+			return;
+		}
+		Planner p(h);
+		size_t i = 0;
+		try {
+			while(i < count) {
+				const tmfqs_op &op = ops[i];
+				validate_op(h, op);
+				if(op.kind == TMFQS_OP_SWAP) {
+					const size_t run = swap_run(ops, i, count);
+					if(run >= 2) {
+						for(size_t j = i; j < i + run; ++j) validate_op(h, ops[j]);
+						p.flush();
+						std::vector<std::pair<unsigned, unsigned>> pairs;
+						for(size_t j = i; j < i + run; ++j) pairs.push_back({bit_of(h, ops[j].q0), bit_of(h, ops[j].q1)});
+						{
+							PassTimer timer(h, TMFQS_KT_PERMUTE, sweep_bytes(h));
+							tqb::launch_bit_permutation(ctx(h), h->precision, h->amps, h->n, pairs);
+						}
+						++h->stats.fused_passes;
+						i += run;
+						continue;
+					}
+				}
+				if(op.kind == TMFQS_OP_GATE) {
+					p.flush();
+					run_gate(h, op.matrix, op.qubits, op.k);
+					++i;
+					continue;
+				}
+				p.add(op);
+				++i;
+			}
+			p.flush();
+		} catch(const tqb::Error &) {
+			// Ops before the failing one are applied, as in the reference's
+			// sequential loop (simulator.cpp:72-82).
+			p.flush();
+			throw;
+		}
+		check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
+	});
+}
+
+int tmfqs_gpu_grover_run(tmfqs_gpu_state *h, tmfqs_register_view *view, const uint64_t *marked, size_t count,
+                         uint64_t iterations, int materialized) {
+	return guarded([&] {
+		ensure_initialized(h, "grover");
+		if(!view) fail(TMFQS_ERR_INVALID_ARGUMENT, "null register view");
+		if(count && !marked) fail(TMFQS_ERR_INVALID_ARGUMENT, "null marked list");
+		std::vector<uint64_t> mk(marked, marked + count);
+		std::sort(mk.begin(), mk.end());
+		mk.erase(std::unique(mk.begin(), mk.end()), mk.end());
+		for(uint64_t s : mk) validate_state(h, s, "QuantumRegister::applyPhaseFlipBasisState");
+		DeviceScope d(h);
+		if(iterations == 0) return;
+		if(materialized && h->opt_grover_fusion && !view->overlay) {
+			if(h->precision == TMFQS_FP64) grover_materialized_fused<double>(h, view, mk, iterations);
+			else grover_materialized_fused<float>(h, view, mk, iterations);
+			return;
+		}
+		for(uint64_t k = 0; k < iterations; ++k) {
+			for(uint64_t s : mk) register_flip(h, view, s);
+			register_inversion(h, view, materialized != 0);
+		}
+		check_cuda(cudaStreamSynchronize(h->stream), "grover sync");
+	});
+}
+
+int tmfqs_gpu_sync(tmfqs_gpu_state *h) {
+	return guarded([&] {
+		require_handle(h);
+		DeviceScope d(h);
+		flush_dirty(h);
+		check_cuda(cudaStreamSynchronize(h->stream), "sync");
+	});
+}
+
+int tmfqs_gpu_stats(tmfqs_gpu_state *h, tmfqs_stats *out) {
+	return guarded([&] {
+		require_handle(h);
+		*out = h->stats;
+	});
+}
+
+int tmfqs_gpu_reset_stats(tmfqs_gpu_state *h) {
+	return guarded([&] {
+		require_handle(h);
+		DeviceScope d(h);
+		resolve_timers(h);
+		h->stats = tmfqs_stats{};
+		for(auto &t : h->times) t = tmfqs_kernel_time{};
+	});
+}
+
+int tmfqs_gpu_kernel_times(tmfqs_gpu_state *h, tmfqs_kernel_time *out) {
+	return guarded([&] {
+		require_handle(h);
+		if(!out) fail(TMFQS_ERR_INVALID_ARGUMENT, "null output");
+		DeviceScope d(h);
+		resolve_timers(h);
+		for(int i = 0; i < TMFQS_KT_COUNT; ++i) out[i] = h->times[i];
+	});
+}
+
+int tmfqs_gpu_set_option(tmfqs_gpu_state *h, int option, long value) {
+	return guarded([&] {
+		require_handle(h);
+		switch(option) {
+			case TMFQS_OPT_FUSION: h->opt_fusion = value != 0; break;
+			case TMFQS_OPT_FUSED_QUBITS:
+				if(value < 0 || value > 10) fail(TMFQS_ERR_INVALID_ARGUMENT, "fused qubits must be in [0, 10]");
+				h->opt_fused_qubits = (int)value;
+				break;
+			case TMFQS_OPT_GROVER_FUSION: h->opt_grover_fusion = value != 0; break;
+			case TMFQS_OPT_KERNEL_TIMING: h->opt_timing = value != 0; break;
+			default: fail(TMFQS_ERR_INVALID_ARGUMENT, "unknown option");
+		}
+	});
+}
+
+int tmfqs_gpu_device_buffer(tmfqs_gpu_state *h, void **ptr, size_t *bytes) {
+	return guarded([&] {
+		ensure_initialized(h, "device buffer query");
+		flush_dirty(h);
+		h->cache.clear();
+		*ptr = h->amps;
+		*bytes = h->bytes;
+	});
+}
+
+int tmfqs_gpu_stream(tmfqs_gpu_state *h, void **stream) {
+	return guarded([&] {
+		require_handle(h);
+		*stream = h->stream;
+	});
+}
+
+}  // extern "C"

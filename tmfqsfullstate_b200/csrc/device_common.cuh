@@ -1,0 +1,60 @@
+// Device-side helpers shared by the kernels of libtmfqs_b200.
+//
+// Exactness: every kernel that must match the reference uses the explicit
+// round-to-nearest intrinsics below (no FMA contraction; the library is also
+// compiled with -fmad=false), so each complex operation is the same sequence
+// of IEEE operations as the reference C++ expression it restates.
+#ifndef TMFQS_B200_DEVICE_COMMON_CUH
+#define TMFQS_B200_DEVICE_COMMON_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tqb {
+
+template <typename R>
+struct Vec2;
+template <>
+struct Vec2<double> {
+	typedef double2 type;
+};
+template <>
+struct Vec2<float> {
+	typedef float2 type;
+};
+
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+
+// Insert a zero bit at position b of i.
+__device__ __forceinline__ uint64_t insert0(uint64_t i, unsigned b) {
+	const uint64_t lo = i & ((1ull << b) - 1ull);
+	return ((i ^ lo) << 1) | lo;
+}
+
+// Insert zero bits at positions lo < hi.
+__device__ __forceinline__ uint64_t insert00(uint64_t i, unsigned lo, unsigned hi) {
+	return insert0(insert0(i, lo), hi);
+}
+
+// Complex product (pr + i pi) * (re + i im) as written in
+// dense_state_backend.cpp:300-301: re' = pr*re - pi*im; im' = pr*im + pi*re.
+template <typename R>
+__device__ __forceinline__ void cmul_ref(R pr, R pi, R &re, R &im) {
+	const R nr = rsub(rmul(pr, re), rmul(pi, im));
+	const R ni = radd(rmul(pr, im), rmul(pi, re));
+	re = nr;
+	im = ni;
+}
+
+// Grid-stride helpers.
+__device__ __forceinline__ uint64_t gtid() { return (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint64_t gstride() { return (uint64_t)gridDim.x * blockDim.x; }
+
+}  // namespace tqb
+
+#endif

@@ -1,0 +1,181 @@
+// Internal interfaces of libtmfqs_b200: the handle, kernel launchers, and the
+// fused-pass program format.  Not part of the public C ABI.
+#ifndef TMFQS_B200_INTERNAL_H
+#define TMFQS_B200_INTERNAL_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/tmfqs_b200.h"
+
+namespace tqb {
+
+// ---------------------------------------------------------------------------
+// Errors: launchers throw Error; the C ABI converts it to a status code.
+// ---------------------------------------------------------------------------
+struct Error {
+	int status;
+	std::string message;
+};
+
+[[noreturn]] void fail(int status, const std::string &message);
+void check_cuda(cudaError_t e, const char *what);
+
+// ---------------------------------------------------------------------------
+// Exact sequential-sum engine (seqsum.cu)
+// ---------------------------------------------------------------------------
+enum TermKind { kTermProb = 0, kTermReal = 1, kTermImag = 2 };
+
+struct Overlay {
+	bool active = false;
+	double sre = 1.0, sim = 0.0, bre = 0.0, bim = 0.0;
+};
+
+struct SeqScratch {
+	void *base = nullptr;  // one device allocation, carved below
+	size_t bytes = 0;
+	uint64_t tiles = 0, groups = 0;
+	void *tile_a = nullptr, *tile_pre = nullptr, *tile_b = nullptr;
+	void *group_a = nullptr, *group_pre = nullptr, *group_b = nullptr;
+	void *walk_out = nullptr;  // WalkOut
+	void *host_out = nullptr;  // pinned WalkOut mirror
+};
+
+struct SeqResult {
+	uint64_t index;  // first index whose running sum reaches the threshold, or N
+	double value;    // running sum at that index (or the full sum)
+};
+
+// Computes the reference's left-to-right double sum of term(j), j < N, or
+// with stop=true the first j whose running sum reaches rnd.  Synchronises.
+SeqResult seq_replay(int precision, const void *amps, uint64_t N, TermKind kind, const Overlay &ov, bool stop,
+                     double rnd, SeqScratch &scratch, cudaStream_t stream, int num_sms, uint64_t *launches);
+void seq_scratch_free(SeqScratch &scratch);
+
+// ---------------------------------------------------------------------------
+// Single-operation kernels (gates.cu)
+// ---------------------------------------------------------------------------
+struct LaunchCtx {
+	cudaStream_t stream;
+	int num_sms;
+	uint64_t *launches;
+};
+
+void launch_h(const LaunchCtx &c, int prec, void *a, unsigned n, unsigned bit);
+void launch_x(const LaunchCtx &c, int prec, void *a, unsigned n, unsigned bit);
+void launch_cnot(const LaunchCtx &c, int prec, void *a, unsigned n, unsigned cbit, unsigned tbit);
+void launch_cphase(const LaunchCtx &c, int prec, void *a, unsigned n, unsigned cbit, unsigned tbit, double cr,
+                   double ci);
+void launch_swap(const LaunchCtx &c, int prec, void *a, unsigned n, unsigned abit, unsigned bbit);
+void launch_phase_flip(const LaunchCtx &c, int prec, void *a, uint64_t s);
+void launch_inversion(const LaunchCtx &c, int prec, void *a, unsigned n, double two_mre, double two_mim);
+void launch_affine(const LaunchCtx &c, int prec, void *a, unsigned n, double sre, double sim, double bre,
+                   double bim);
+void launch_scatter_uniform(const LaunchCtx &c, int prec, void *a, const uint64_t *states, uint64_t count,
+                            double amp);
+void launch_scatter_values(const LaunchCtx &c, int prec, void *a, const uint64_t *idx, const double *vals,
+                           uint64_t count);
+// matrix: device, row-major 2^k x 2^k interleaved complex (double);
+// tpos: device array of the k target bit positions in block order.
+void launch_gate(const LaunchCtx &c, int prec, void *a, unsigned n, unsigned k, const double *matrix,
+                 const unsigned *tpos_host);
+// complex128 <-> complex64 conversion of `count` amplitudes (device buffers).
+void launch_to_c64(const LaunchCtx &c, void *dst, const double *src, uint64_t count);
+void launch_from_c64(const LaunchCtx &c, double *dst, const void *src, uint64_t count);
+
+// ---------------------------------------------------------------------------
+// Fused multi-gate passes (fused.cu)
+// ---------------------------------------------------------------------------
+enum FusedOpKind : uint32_t {
+	kFH = 0,       // Hadamard on local bit
+	kFHChain = 1,  // Hadamard on local bit, then a chain of controlled phases on its |1> half
+	kFX = 2,       // Pauli-X on local bit
+	kFCnot = 3,    // CNOT: local target bit, global control mask
+	kFCP = 4,      // controlled phase, any two bits (diagonal)
+	kFFlip = 5,    // phase flip of one basis state (diagonal)
+	kFSwap = 6     // swap of two local bits
+};
+
+struct FusedOp {
+	uint32_t kind;
+	uint32_t lt;     // local target bit (H, HChain, X, CNOT, Swap first)
+	uint32_t lc;     // Swap second local bit
+	uint32_t tab;    // HChain: offset of its phase table in FusedPass::phases (64 entries per chain)
+	uint64_t mask;   // CNOT: control mask; CP: both bit masks; HChain: mask of chain control bits
+	uint64_t state;  // Flip state
+	double cr, ci;   // CP phase
+};
+
+struct FusedPass {
+	unsigned n = 0;
+	unsigned K = 0;                 // local bits (tile = 2^K amplitudes)
+	unsigned lpos[16] = {0};        // global bit position of local bit i, ascending
+	std::vector<FusedOp> ops;
+	std::vector<double> phases;     // HChain tables: 64 x (cos, sin) per chain, indexed by bit position
+	unsigned gate_count = 0;        // circuit operations folded into this pass
+};
+
+// Runs one fused pass over the whole state.  `dev_prog` is a device buffer
+// the launcher may (re)use for the program.
+void launch_fused_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, void *&dev_prog,
+                       size_t &dev_prog_bytes);
+
+// Involutive permutation of bit positions (disjoint transpositions), as one
+// in-place pass: amplitude x moves to perm(x).  pairs[i] = (p, q) bit positions.
+void launch_bit_permutation(const LaunchCtx &c, int prec, void *a, unsigned n,
+                            const std::vector<std::pair<unsigned, unsigned>> &pairs);
+
+// Materialised Grover iterations as one temporal pass: for k in [0,K):
+// flip marked states, then a <- two_mean[k] - a (exact per-iteration ops).
+// Marked states are flipped from iteration `flip_from` on (the first
+// iteration's flips may already have been applied when its mean was taken).
+void launch_grover_temporal(const LaunchCtx &c, int prec, void *a, unsigned n, const double *dev_two_means,
+                            uint64_t iterations, const uint64_t *dev_marked, unsigned marked_count,
+                            uint64_t flip_from);
+
+}  // namespace tqb
+
+// ---------------------------------------------------------------------------
+// The handle.
+// ---------------------------------------------------------------------------
+struct tmfqs_gpu_state {
+	int device = 0;
+	int precision = TMFQS_FP64;
+	int num_sms = 148;
+	unsigned n = 0;
+	uint64_t N = 0;
+	bool initialized = false;
+	void *amps = nullptr;
+	size_t bytes = 0;
+	cudaStream_t stream = nullptr;
+	tqb::SeqScratch seq;
+	// Host cache of single amplitudes (amplitude / setAmplitude / phase flips
+	// of cached states); dirty entries are flushed before any kernel runs.
+	std::unordered_map<uint64_t, std::pair<double, double>> cache;
+	std::unordered_map<uint64_t, bool> dirty;
+	double *pinned = nullptr;  // small pinned staging buffer
+	size_t pinned_elems = 0;
+	void *dev_small = nullptr;  // small device staging buffer
+	size_t dev_small_bytes = 0;
+	void *dev_prog = nullptr;
+	size_t dev_prog_bytes = 0;
+	tmfqs_stats stats{};
+	// Kernel timing (TMFQS_OPT_KERNEL_TIMING): event pairs per class, resolved lazily.
+	bool opt_timing = false;
+	struct TimedLaunch {
+		int kind;
+		cudaEvent_t start, stop;
+		double bytes;
+	};
+	std::vector<TimedLaunch> timed;
+	tmfqs_kernel_time times[TMFQS_KT_COUNT] = {};
+	bool opt_fusion = true;
+	int opt_fused_qubits = 0;  // 0 = default by precision
+	bool opt_grover_fusion = true;
+};
+
+#endif
