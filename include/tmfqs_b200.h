@@ -102,7 +102,11 @@ typedef enum {
 	TMFQS_OPT_FUSION = 0,        /* 1 (default): apply_ops fuses gates into multi-gate passes */
 	TMFQS_OPT_FUSED_QUBITS = 1,  /* target qubits per fused pass (default 9) */
 	TMFQS_OPT_GROVER_FUSION = 2, /* 1 (default): Grover runs execute as one temporal pass */
-	TMFQS_OPT_KERNEL_TIMING = 3  /* 1: time every pass with CUDA events on the handle's stream */
+	TMFQS_OPT_KERNEL_TIMING = 3, /* 1: time every pass with CUDA events on the handle's stream */
+	TMFQS_OPT_EXACT = 4          /* FP64 handles: 1 (default) bit-identical controlled-phase chains;
+	                                0: each chain as one twiddle per amplitude from FP64 tables
+	                                (about 1e-15 relative error per pass).  FP32 handles always
+	                                use twiddles. */
 } tmfqs_option;
 
 /* Kernel classes for tmfqs_gpu_kernel_times. */

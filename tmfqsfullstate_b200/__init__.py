@@ -102,6 +102,7 @@ class KernelTime(ctypes.Structure):
 
 KT_NAMES = ("fused", "permute", "gate", "reduce", "grover")
 OPT_KERNEL_TIMING = 3
+OPT_EXACT = 4
 
 
 class Stats(ctypes.Structure):

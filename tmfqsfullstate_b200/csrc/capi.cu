@@ -289,7 +289,6 @@ struct Planner {
 	tqb::FusedPass pass;
 	uint64_t tmask = 0;  // bits that must be local (moving bits of ops in the pass)
 	int chain_op = -1;   // index of the H-chain op that may still grow
-	unsigned chain_low = 64;  // lowest bit position in that chain so far
 	size_t nontrivial = 0;
 	std::vector<const tmfqs_op *> pending;  // circuit ops in the pass (for single-op fallback)
 
@@ -306,7 +305,6 @@ struct Planner {
 		pass.n = h->n;
 		tmask = 0;
 		chain_op = -1;
-		chain_low = 64;
 		nontrivial = 0;
 		pending.clear();
 	}
@@ -336,6 +334,21 @@ struct Planner {
 		for(unsigned i = 0; i < pass.K; ++i) pass.lpos[i] = L[i];
 	}
 
+	// A chain becomes a twiddle when its local controls are distinct and fit
+	// the two per-tile tables (6 + 5 bits); outer controls are unlimited.
+	bool twiddle_ok(const tqb::FusedOp &op) const {
+		uint32_t seen = 0;
+		unsigned locals = 0;
+		for(unsigned e = 0; e < op.lc; ++e) {
+			const auto &ce = pass.chain[op.tab + e];
+			if(ce.local < 0) continue;
+			if(seen & (1u << ce.local)) return false;
+			seen |= 1u << ce.local;
+			++locals;
+		}
+		return locals <= 11;
+	}
+
 	// Ops are recorded with global bit positions in `lt`/`lc` and converted to
 	// local indices once the local set is known.
 	void flush() {
@@ -344,8 +357,16 @@ struct Planner {
 			run_single(*pending[0]);
 		} else {
 			finalize_local_set();
+			for(auto &e : pass.chain) {
+				e.local = -1;
+				for(unsigned i = 0; i < pass.K; ++i)
+					if(pass.lpos[i] == e.bit) e.local = (int32_t)i;
+			}
+			const bool twiddle = !h->opt_exact || h->precision == TMFQS_FP32;
 			for(auto &op : pass.ops) {
-				if(op.kind == tqb::kFH || op.kind == tqb::kFHChain || op.kind == tqb::kFX || op.kind == tqb::kFCnot)
+				if(op.kind == tqb::kFHChain && twiddle && twiddle_ok(op)) op.kind = tqb::kFHTwiddle;
+				if(op.kind == tqb::kFH || op.kind == tqb::kFHChain || op.kind == tqb::kFHTwiddle || op.kind == tqb::kFX ||
+				   op.kind == tqb::kFCnot)
 					op.lt = local_index(op.lt);
 				if(op.kind == tqb::kFSwap) {
 					op.lt = local_index(op.lt);
@@ -392,7 +413,6 @@ struct Planner {
 		if(kind == tqb::kFH) {
 			// A Hadamard may grow into an H-chain with the phases that follow.
 			chain_op = (int)pass.ops.size() - 1;
-			chain_low = bit;
 		}
 	}
 
@@ -422,16 +442,16 @@ struct Planner {
 					tqb::FusedOp &ch = pass.ops[chain_op];
 					const unsigned hb = ch.lt;  // global bit of the chain's Hadamard
 					const int other = bc == hb ? (int)bt : (bt == hb ? (int)bc : -1);
-					if(other >= 0 && (unsigned)other < chain_low) {
+					// Any controlled phase on the Hadamard's qubit that directly follows
+					// it acts only on the butterflies' |1> outputs: append it to the chain.
+					if(other >= 0 && ch.lc < 64) {
 						if(ch.kind == tqb::kFH) {
 							ch.kind = tqb::kFHChain;
-							ch.tab = (uint32_t)(pass.phases.size() / 2);
-							pass.phases.resize(pass.phases.size() + 128, 0.0);
+							ch.tab = (uint32_t)pass.chain.size();
+							ch.lc = 0;
 						}
-						ch.mask |= 1ull << other;
-						pass.phases[2 * (ch.tab + other)] = cr;
-						pass.phases[2 * (ch.tab + other) + 1] = ci;
-						chain_low = (unsigned)other;
+						pass.chain.push_back(tqb::ChainEntry{cr, ci, op.theta, -1, (uint32_t)other});
+						++ch.lc;
 						pending.push_back(&op);
 						return;
 					}
@@ -765,6 +785,7 @@ int tmfqs_gpu_clone(tmfqs_gpu_state *h, tmfqs_gpu_state **out) {
 			c->opt_fusion = h->opt_fusion;
 			c->opt_fused_qubits = h->opt_fused_qubits;
 			c->opt_grover_fusion = h->opt_grover_fusion;
+			c->opt_exact = h->opt_exact;
 			if(h->initialized) {
 				flush_dirty(h);
 				ensure_state(c, h->n);
@@ -1246,6 +1267,7 @@ int tmfqs_gpu_set_option(tmfqs_gpu_state *h, int option, long value) {
 				break;
 			case TMFQS_OPT_GROVER_FUSION: h->opt_grover_fusion = value != 0; break;
 			case TMFQS_OPT_KERNEL_TIMING: h->opt_timing = value != 0; break;
+			case TMFQS_OPT_EXACT: h->opt_exact = value != 0; break;
 			default: fail(TMFQS_ERR_INVALID_ARGUMENT, "unknown option");
 		}
 	});

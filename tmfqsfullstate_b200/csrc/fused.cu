@@ -46,26 +46,44 @@ __device__ __forceinline__ uint64_t expand_outer(uint64_t o, const FusedGeom &g)
 }
 
 template <typename R>
-__device__ __forceinline__ void apply_chain(R &re, R &im, uint64_t gidx, uint64_t mask, const double2 *tab) {
-	uint64_t bits = gidx & mask;
-	while(bits) {
-		const unsigned b = 63u - (unsigned)__clzll((long long)bits);
-		bits ^= 1ull << b;
-		if(re == R(0) && im == R(0)) continue;
-		const double2 ph = tab[b];
-		cmul_ref((R)ph.x, (R)ph.y, re, im);
-	}
+__device__ __forceinline__ bool is_zero(typename Vec2<R>::type v) {
+	return v.x == R(0) && v.y == R(0);
+}
+
+// Hadamard butterfly of dense_state_backend.cpp:265-271 (skips all-zero pairs).
+template <typename R>
+__device__ __forceinline__ bool butterfly(typename Vec2<R>::type &x, typename Vec2<R>::type &y, R inv) {
+	if(is_zero<R>(x) && is_zero<R>(y)) return false;
+	typename Vec2<R>::type o0, o1;
+	o0.x = rmul(radd(x.x, y.x), inv);
+	o0.y = rmul(radd(x.y, y.y), inv);
+	o1.x = rmul(rsub(x.x, y.x), inv);
+	o1.y = rmul(rsub(x.y, y.y), inv);
+	x = o0;
+	y = o1;
+	return true;
 }
 
 template <typename R>
 __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type *a, FusedGeom g, const FusedOp *ops,
-                                                         const double2 *phases) {
+                                                         const ChainEntry *chain) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ unsigned char smem_raw[];
 	const unsigned T = 1u << g.K;
 	V *s = reinterpret_cast<V *>(smem_raw);
 	uint64_t *hitab = reinterpret_cast<uint64_t *>(s + T);
 	const unsigned nhi = 1u << (g.K - g.m);
+	// Per-tile compacted chain of the current H-chain op: its entries whose
+	// other bit is local (applied when that bit is set) or an outer bit that
+	// is set in this tile (applied to every |1> output).
+	__shared__ double2 cph[64];
+	__shared__ int cloc[64];
+	__shared__ unsigned ccount;
+	// Twiddle form: table A (outer phase x first 6 local controls) and table B
+	// (next 5 local controls), built per tile in FP64.
+	__shared__ double2 twa[64], twb[32];
+	__shared__ int tla[6], tlb[5];
+	__shared__ int tna, tnb;
 	for(unsigned h = threadIdx.x; h < nhi; h += blockDim.x) {
 		uint64_t v = 0;
 		for(unsigned i = 0; i < g.K - g.m; ++i)
@@ -73,9 +91,11 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 		hitab[h] = v;
 	}
 	__syncthreads();
+	const unsigned lane = threadIdx.x & 31u;
 	const unsigned lowmask = (1u << g.m) - 1u;
 	auto scatter = [&](unsigned j) -> uint64_t { return (uint64_t)(j & lowmask) | hitab[j >> g.m]; };
 	const unsigned half = T >> 1, quarter = T >> 2;
+	const R inv = (R)g.inv;
 	for(uint64_t o = blockIdx.x; o < g.ntiles; o += gridDim.x) {
 		const uint64_t base = expand_outer(o, g);
 		for(unsigned j = threadIdx.x; j < T; j += blockDim.x) s[j] = a[base | scatter(j)];
@@ -83,21 +103,160 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 		for(unsigned k = 0; k < g.nops; ++k) {
 			const FusedOp op = ops[k];
 			switch(op.kind) {
-				case kFH:
-				case kFHChain: {
-					const R inv = (R)g.inv;
+				case kFH: {
 					for(unsigned p = threadIdx.x; p < half; p += blockDim.x) {
 						const unsigned j0 = (unsigned)insert0(p, op.lt), j1 = j0 | (1u << op.lt);
-						const V x = s[j0], y = s[j1];
-						if(x.x == R(0) && x.y == R(0) && y.x == R(0) && y.y == R(0)) continue;
-						V o0, o1;
-						o0.x = rmul(radd(x.x, y.x), inv);
-						o0.y = rmul(radd(x.y, y.y), inv);
-						o1.x = rmul(rsub(x.x, y.x), inv);
-						o1.y = rmul(rsub(x.y, y.y), inv);
-						if(op.kind == kFHChain) apply_chain<R>(o1.x, o1.y, base | scatter(j1), op.mask, phases + op.tab);
-						s[j0] = o0;
-						s[j1] = o1;
+						V x = s[j0], y = s[j1];
+						if(!butterfly<R>(x, y, inv)) continue;
+						s[j0] = x;
+						s[j1] = y;
+					}
+					__syncthreads();
+					break;
+				}
+				case kFHChain: {
+					if(threadIdx.x < 32) {
+						unsigned pos = 0;
+						for(unsigned e0 = 0; e0 < op.lc; e0 += 32) {
+							const unsigned e = e0 + lane;
+							bool keep = false;
+							ChainEntry ce{};
+							if(e < op.lc) {
+								ce = chain[op.tab + e];
+								keep = ce.local >= 0 || ((base >> ce.bit) & 1ull);
+							}
+							const unsigned m = __ballot_sync(0xffffffffu, keep);
+							const unsigned off = pos + __popc(m & ((1u << lane) - 1u));
+							if(keep) {
+								cph[off] = make_double2(ce.cr, ce.ci);
+								cloc[off] = ce.local;
+							}
+							pos += __popc(m);
+						}
+						if(lane == 0) ccount = pos;
+					}
+					__syncthreads();
+					const unsigned cnt = ccount;
+					// Two butterflies per iteration: their chains are independent and
+					// see the same tile-uniform outer phases (ILP).
+					for(unsigned p0 = threadIdx.x; p0 < half; p0 += 2 * blockDim.x) {
+						const unsigned p1 = p0 + blockDim.x;
+						const bool has1 = p1 < half;
+						const unsigned j00 = (unsigned)insert0(p0, op.lt), j01 = j00 | (1u << op.lt);
+						const unsigned j10 = has1 ? (unsigned)insert0(p1, op.lt) : j00, j11 = j10 | (1u << op.lt);
+						V x0 = s[j00], y0 = s[j01], x1 = s[j10], y1 = s[j11];
+						const bool w0 = butterfly<R>(x0, y0, inv);
+						const bool w1 = has1 && butterfly<R>(x1, y1, inv);
+						// A zero |1> output is left alone by every phase of the chain
+						// (dense_state_backend.cpp:299); a nonzero one stays nonzero.
+						const bool c0 = w0 && !is_zero<R>(y0), c1 = w1 && !is_zero<R>(y1);
+						if(c0 || c1) {
+							R r0 = y0.x, i0 = y0.y, r1 = y1.x, i1 = y1.y;
+							for(unsigned e = 0; e < cnt; ++e) {
+								const double2 ph = cph[e];
+								const int l = cloc[e];
+								R pr0 = (R)ph.x, pi0 = (R)ph.y, pr1 = pr0, pi1 = pi0;
+								if(l >= 0) {
+									// Multiplying by (1, 0) leaves a value unchanged exactly.
+									if(!((j01 >> l) & 1u)) {
+										pr0 = R(1);
+										pi0 = R(0);
+									}
+									if(!((j11 >> l) & 1u)) {
+										pr1 = R(1);
+										pi1 = R(0);
+									}
+								}
+								cmul_ref(pr0, pi0, r0, i0);
+								cmul_ref(pr1, pi1, r1, i1);
+							}
+							if(c0) {
+								y0.x = r0;
+								y0.y = i0;
+							}
+							if(c1) {
+								y1.x = r1;
+								y1.y = i1;
+							}
+						}
+						if(w0) {
+							s[j00] = x0;
+							s[j01] = y0;
+						}
+						if(w1) {
+							s[j10] = x1;
+							s[j11] = y1;
+						}
+					}
+					__syncthreads();
+					break;
+				}
+				case kFHTwiddle: {
+					if(threadIdx.x < 96) {
+						double outer = 0.0;
+						int nl = 0;
+						int lidx[11];
+						double lth[11];
+						for(unsigned e = 0; e < op.lc; ++e) {
+							const ChainEntry ce = chain[op.tab + e];
+							if(ce.local < 0) {
+								if((base >> ce.bit) & 1ull) outer += ce.theta;
+							} else if(nl < 11) {
+								lidx[nl] = ce.local;
+								lth[nl] = ce.theta;
+								++nl;
+							}
+						}
+						const int na = nl < 6 ? nl : 6, nb = nl - na;
+						double ang = 0.0;
+						bool active = false;
+						unsigned m = 0;
+						if(threadIdx.x < 64) {
+							m = threadIdx.x;
+							active = m < (1u << na);
+							ang = outer;
+							for(int i = 0; i < na; ++i)
+								if((m >> i) & 1u) ang += lth[i];
+						} else {
+							m = threadIdx.x - 64;
+							active = m < (1u << nb);
+							for(int i = 0; i < nb; ++i)
+								if((m >> i) & 1u) ang += lth[na + i];
+						}
+						if(active) {
+							double sv, cv;
+							sincos(ang, &sv, &cv);
+							if(threadIdx.x < 64) twa[m] = make_double2(cv, sv);
+							else twb[m] = make_double2(cv, sv);
+						}
+						if(threadIdx.x == 0) {
+							for(int i = 0; i < na; ++i) tla[i] = lidx[i];
+							for(int i = 0; i < nb; ++i) tlb[i] = lidx[na + i];
+							tna = na;
+							tnb = nb;
+						}
+					}
+					__syncthreads();
+					const int na = tna, nb = tnb;
+					for(unsigned p = threadIdx.x; p < half; p += blockDim.x) {
+						const unsigned j0 = (unsigned)insert0(p, op.lt), j1 = j0 | (1u << op.lt);
+						V x = s[j0], y = s[j1];
+						if(!butterfly<R>(x, y, inv)) continue;
+						if(!is_zero<R>(y)) {
+							unsigned ia = 0, ib = 0;
+							for(int i = 0; i < na; ++i) ia |= ((j1 >> tla[i]) & 1u) << i;
+							for(int i = 0; i < nb; ++i) ib |= ((j1 >> tlb[i]) & 1u) << i;
+							const double2 ta = twa[ia], tb = twb[ib];
+							// Twiddle formed in FP64 and rounded once to the storage type.
+							const R tr = (R)fma(ta.x, tb.x, -(ta.y * tb.y));
+							const R ti = (R)fma(ta.x, tb.y, ta.y * tb.x);
+							const R nr = fma(tr, y.x, -(ti * y.y));
+							const R ni = fma(tr, y.y, ti * y.x);
+							y.x = nr;
+							y.y = ni;
+						}
+						s[j0] = x;
+						s[j1] = y;
 					}
 					__syncthreads();
 					break;
@@ -315,7 +474,7 @@ void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	g.inv = 1.0 / std::sqrt(2.0);
 	const size_t ops_bytes = pass.ops.size() * sizeof(FusedOp);
 	const size_t ph_off = (ops_bytes + 255) & ~size_t(255);
-	const size_t need = ph_off + std::max<size_t>(16, pass.phases.size() * sizeof(double));
+	const size_t need = ph_off + std::max<size_t>(32, pass.chain.size() * sizeof(ChainEntry));
 	if(need > dev_prog_bytes) {
 		if(dev_prog) {
 			check_cuda(cudaStreamSynchronize(c.stream), "fused program sync");
@@ -332,7 +491,7 @@ void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	// The program buffer is reused: make sure the previous pass consumed it.
 	std::vector<unsigned char> host(need, 0);
 	std::memcpy(host.data(), pass.ops.data(), ops_bytes);
-	if(!pass.phases.empty()) std::memcpy(host.data() + ph_off, pass.phases.data(), pass.phases.size() * sizeof(double));
+	if(!pass.chain.empty()) std::memcpy(host.data() + ph_off, pass.chain.data(), pass.chain.size() * sizeof(ChainEntry));
 	check_cuda(cudaMemcpyAsync(dev_prog, host.data(), need, cudaMemcpyHostToDevice, c.stream), "fused program upload");
 	check_cuda(cudaStreamSynchronize(c.stream), "fused program upload sync");
 	const size_t smem = (sizeof(typename Vec2<R>::type) << pass.K) + (sizeof(uint64_t) << (pass.K - g.m));
@@ -342,7 +501,7 @@ void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	const uint64_t grid = std::min<uint64_t>(g.ntiles, (uint64_t)c.num_sms * std::max(1, per_sm));
 	k_fused<R><<<(unsigned)grid, kFusedThreads, smem, c.stream>>>(
 		static_cast<typename Vec2<R>::type *>(a), g, static_cast<const FusedOp *>(dev_prog),
-		reinterpret_cast<const double2 *>(static_cast<unsigned char *>(dev_prog) + ph_off));
+		reinterpret_cast<const ChainEntry *>(static_cast<unsigned char *>(dev_prog) + ph_off));
 	after_launch(c, "fused pass");
 }
 

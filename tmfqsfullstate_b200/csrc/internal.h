@@ -97,17 +97,27 @@ enum FusedOpKind : uint32_t {
 	kFCnot = 3,    // CNOT: local target bit, global control mask
 	kFCP = 4,      // controlled phase, any two bits (diagonal)
 	kFFlip = 5,    // phase flip of one basis state (diagonal)
-	kFSwap = 6     // swap of two local bits
+	kFSwap = 6,    // swap of two local bits
+	kFHTwiddle = 7 // Hadamard, then its H-chain applied as one twiddle per |1> output
 };
 
 struct FusedOp {
 	uint32_t kind;
 	uint32_t lt;     // local target bit (H, HChain, X, CNOT, Swap first)
-	uint32_t lc;     // Swap second local bit
-	uint32_t tab;    // HChain: offset of its phase table in FusedPass::phases (64 entries per chain)
-	uint64_t mask;   // CNOT: control mask; CP: both bit masks; HChain: mask of chain control bits
+	uint32_t lc;     // Swap: second local bit; HChain: number of chain entries
+	uint32_t tab;    // HChain: index of its first entry in FusedPass::chain
+	uint64_t mask;   // CNOT: control mask; CP: both bit masks
 	uint64_t state;  // Flip state
 	double cr, ci;   // CP phase
+};
+
+// One controlled phase of an H-chain, in circuit order (bit positions
+// strictly descending along a chain).
+struct ChainEntry {
+	double cr, ci;   // cos(theta), sin(theta) from the host C library
+	double theta;    // the angle itself (twiddle form)
+	int32_t local;   // local bit index of the other qubit, or -1 if it is an outer bit
+	uint32_t bit;    // global bit position of the other qubit
 };
 
 struct FusedPass {
@@ -115,7 +125,7 @@ struct FusedPass {
 	unsigned K = 0;                 // local bits (tile = 2^K amplitudes)
 	unsigned lpos[16] = {0};        // global bit position of local bit i, ascending
 	std::vector<FusedOp> ops;
-	std::vector<double> phases;     // HChain tables: 64 x (cos, sin) per chain, indexed by bit position
+	std::vector<ChainEntry> chain;  // H-chain entries of all chains of the pass
 	unsigned gate_count = 0;        // circuit operations folded into this pass
 };
 
@@ -176,6 +186,7 @@ struct tmfqs_gpu_state {
 	bool opt_fusion = true;
 	int opt_fused_qubits = 0;  // 0 = default by precision
 	bool opt_grover_fusion = true;
+	bool opt_exact = true;  // FP64: bit-identical chains (false: one twiddle per |1> output)
 };
 
 #endif
