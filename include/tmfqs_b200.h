@@ -213,6 +213,22 @@ TMFQS_API int tmfqs_gpu_apply_ops(tmfqs_gpu_state *h, const tmfqs_op *ops, size_
  * updating *view in place (appendGrover, circuit.cpp:118-141). */
 TMFQS_API int tmfqs_gpu_grover_run(tmfqs_gpu_state *h, tmfqs_register_view *view, const uint64_t *marked,
                                    size_t count, uint64_t iterations, int materialized);
+/* No counterpart in the reference.  The exact measurement of
+ * tmfqs_gpu_sample for callers that cannot let the library allocate device
+ * memory -- an application whose own caching allocator already holds nearly
+ * all of HBM, or a loop that must not pay the device-wide synchronisation of
+ * cudaMalloc/cudaFree.  The caller passes its own device state (2^n
+ * interleaved complex amplitudes: complex128 for TMFQS_FP64, complex64 for
+ * TMFQS_FP32), the draw, the CUDA stream to run on (NULL = default stream)
+ * and a host pointer for the index; the function allocates nothing.  Its
+ * working tables live in a fixed 2 MiB device array inside the library, so
+ * states are limited to num_qubits <= 24 (larger ones return
+ * TMFQS_ERR_INVALID_ARGUMENT).  The first call on each device looks up that
+ * array's device address (cudaGetSymbolAddress): make it before any stream
+ * capture.  All calls share the array -- calls that overlap on the GPU race --
+ * and each call returns after the result is on the host. */
+TMFQS_API int tmfqs_sample_static(const void *device_amps, int precision, unsigned num_qubits, double rnd,
+                                  void *stream, uint64_t *index_out);
 /* endOperationBatch, i_state_backend.h:163: waits for all queued work. */
 TMFQS_API int tmfqs_gpu_sync(tmfqs_gpu_state *h);
 

@@ -165,6 +165,7 @@ SIGNATURES = {
     "tmfqs_gpu_device_buffer": [_H, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)],
     "tmfqs_gpu_stream": [_H, ctypes.POINTER(ctypes.c_void_p)],
     "tmfqs_random_phase": [_UI, ctypes.c_uint32, _DP],
+    "tmfqs_sample_static": [ctypes.c_void_p, ctypes.c_int, _UI, _D, ctypes.c_void_p, _U64P],
     "tmfqs_mt19937_unit": [ctypes.c_uint32, _U64, _DP],
 }
 
@@ -270,6 +271,19 @@ def mt19937_unit(seed: int, count: int) -> np.ndarray:
     out = np.empty(count, dtype=np.float64)
     _check(lib().tmfqs_mt19937_unit(seed, count, _dptr(out)))
     return out
+
+
+def sample_static(device_amps: int, precision: int, num_qubits: int, rnd: float, stream: int | None = None) -> int:
+    """Exact measurement over a caller-owned device state without any device allocation.
+
+    For callers that cannot let the library allocate: the working tables use a
+    fixed 2 MiB device array inside libtmfqs_b200 (num_qubits <= 24); calls
+    that overlap on the GPU share it and race.
+    """
+    out = ctypes.c_uint64()
+    _check(lib().tmfqs_sample_static(ctypes.c_void_p(device_amps), precision, num_qubits, rnd,
+                                     ctypes.c_void_p(stream) if stream else None, ctypes.byref(out)))
+    return out.value
 
 
 def op_array(ops):

@@ -1220,6 +1220,19 @@ int tmfqs_gpu_grover_run(tmfqs_gpu_state *h, tmfqs_register_view *view, const ui
 	});
 }
 
+int tmfqs_sample_static(const void *device_amps, int precision, unsigned num_qubits, double rnd, void *stream,
+                        uint64_t *index_out) {
+	return guarded([&] {
+		if(!device_amps || !index_out) fail(TMFQS_ERR_INVALID_ARGUMENT, "tmfqs_sample_static: null pointer");
+		if(precision != TMFQS_FP64 && precision != TMFQS_FP32) fail(TMFQS_ERR_INVALID_ARGUMENT, "unknown precision");
+		if(!(rnd >= 0.0 && rnd < 1.0)) fail(TMFQS_ERR_INVALID_ARGUMENT, "tmfqs_sample_static requires rnd in [0,1)");
+		const tqb::SeqResult r =
+			tqb::seq_sample_static(precision, device_amps, num_qubits, rnd, static_cast<cudaStream_t>(stream));
+		if(r.index >= (1ull << num_qubits)) fail(TMFQS_ERR_RUNTIME, "tmfqs_sample_static: cumulative probability did not reach sample");
+		*index_out = r.index;
+	});
+}
+
 int tmfqs_gpu_sync(tmfqs_gpu_state *h) {
 	return guarded([&] {
 		require_handle(h);

@@ -55,6 +55,9 @@ struct SeqResult {
 SeqResult seq_replay(int precision, const void *amps, uint64_t N, TermKind kind, const Overlay &ov, bool stop,
                      double rnd, SeqScratch &scratch, cudaStream_t stream, int num_sms, uint64_t *launches);
 void seq_scratch_free(SeqScratch &scratch);
+// sampleMeasurement over a caller-owned device state, using the library's
+// fixed device scratch instead of allocating (tmfqs_sample_static).
+SeqResult seq_sample_static(int precision, const void *amps, unsigned num_qubits, double rnd, cudaStream_t stream);
 
 // ---------------------------------------------------------------------------
 // Single-operation kernels (gates.cu)

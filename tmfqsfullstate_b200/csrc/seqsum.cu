@@ -19,6 +19,7 @@
 // small per-tile tables.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "device_common.cuh"
 #include "internal.h"
@@ -562,7 +563,91 @@ void ensure_scratch(SeqScratch &s, uint64_t N) {
 	s.host_out = host;
 }
 
+// ---------------------------------------------------------------------------
+// Fixed device scratch for the allocation-free measurement entry point.
+//
+// Some callers cannot let this library call cudaMalloc: a host application
+// whose caching allocator has already reserved nearly all device memory for
+// itself (so a fresh allocation fails or fragments its pool), or a loop that
+// must not pay the device-wide synchronisation cudaMalloc/cudaFree imply.
+// For them tmfqs_sample_static runs the exact measurement replay with its
+// per-tile tables in this fixed array, which every GPU that loads the library
+// holds until the process exits.  Every region of it is fully written before
+// it is read on each call, so no clearing is needed; calls that overlap on
+// the GPU share the array and race.
+// ---------------------------------------------------------------------------
+constexpr unsigned kStaticMaxQubits = 24;
+constexpr size_t kStaticScratchBytes = size_t(2) << 20;  // 2 MiB
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+std::mutex g_static_mutex;
+void *g_static_addr[64] = {nullptr};  // device address of g_static_scratch, per device ordinal
+
+// Host code cannot use &g_static_scratch as a device address; the runtime
+// gives the real address for the current device.
+void *static_scratch_address() {
+	int dev = 0;
+	check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+	if(dev < 0 || dev >= 64) fail(TMFQS_ERR_INVALID_ARGUMENT, "device ordinal out of range for the static scratch");
+	std::lock_guard<std::mutex> lock(g_static_mutex);
+	if(!g_static_addr[dev]) {
+		void *p = nullptr;
+		check_cuda(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress(static scratch)");
+		g_static_addr[dev] = p;
+	}
+	return g_static_addr[dev];
+}
+
+// Carves the engine's tables out of the static array (same layout as
+// ensure_scratch, without allocating).  Throws if they would not fit.
+void carve_static(SeqScratch &s, uint64_t N, void *base, void *host_out) {
+	const uint64_t tiles = (N + kTile - 1) / kTile;
+	const uint64_t groups = (tiles + kGroup - 1) / kGroup;
+	auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+	const size_t b_ta = align(tiles * sizeof(TileA)), b_tp = align(tiles * sizeof(TilePre)),
+	             b_tb = align(tiles * sizeof(TileB)), b_ga = align(groups * sizeof(GroupA)),
+	             b_gp = align(groups * sizeof(GroupPre)), b_gb = align(groups * sizeof(TileB)),
+	             b_wo = align(sizeof(WalkOut));
+	if(b_ta + b_tp + b_tb + b_ga + b_gp + b_gb + b_wo > kStaticScratchBytes)
+		fail(TMFQS_ERR_INVALID_ARGUMENT, "state too large for the static scratch");
+	char *p = static_cast<char *>(base);
+	s.base = nullptr;  // not owned
+	s.bytes = 0;
+	s.tiles = tiles;
+	s.groups = groups;
+	s.tile_a = p;
+	p += b_ta;
+	s.tile_pre = p;
+	p += b_tp;
+	s.tile_b = p;
+	p += b_tb;
+	s.group_a = p;
+	p += b_ga;
+	s.group_pre = p;
+	p += b_gp;
+	s.group_b = p;
+	p += b_gb;
+	s.walk_out = p;
+	s.host_out = host_out;
+}
+
 }  // namespace
+
+SeqResult seq_sample_static(int precision, const void *amps, unsigned num_qubits, double rnd, cudaStream_t stream) {
+	if(num_qubits > kStaticMaxQubits)
+		fail(TMFQS_ERR_INVALID_ARGUMENT, "tmfqs_sample_static: at most " + std::to_string(kStaticMaxQubits) +
+		                                     " qubits (its fixed " + std::to_string(kStaticScratchBytes >> 20) +
+		                                     " MiB device scratch); use tmfqs_gpu_sample for larger states");
+	const uint64_t N = 1ull << num_qubits;
+	int dev = 0, sms = 0;
+	check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+	check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+	WalkOut host{};  // pageable: the readback copy is synchronous
+	SeqScratch s;
+	carve_static(s, N, static_scratch_address(), &host);
+	if(precision == TMFQS_FP64) return run_engine<double, kTermProb>(amps, N, Overlay{}, true, rnd, s, stream, sms, nullptr);
+	return run_engine<float, kTermProb>(amps, N, Overlay{}, true, rnd, s, stream, sms, nullptr);
+}
 
 void seq_scratch_free(SeqScratch &s) {
 	if(s.base) cudaFree(s.base);
