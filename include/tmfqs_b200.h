@@ -100,13 +100,17 @@ typedef struct {
 /* Tunables (tmfqs_gpu_set_option). */
 typedef enum {
 	TMFQS_OPT_FUSION = 0,        /* 1 (default): apply_ops fuses gates into multi-gate passes */
-	TMFQS_OPT_FUSED_QUBITS = 1,  /* target qubits per fused pass (default 9) */
+	TMFQS_OPT_FUSED_QUBITS = 1,  /* target qubits per fused pass (default: tile bits minus the
+	                                contiguous low bits kept for coalescing) */
 	TMFQS_OPT_GROVER_FUSION = 2, /* 1 (default): Grover runs execute as one temporal pass */
 	TMFQS_OPT_KERNEL_TIMING = 3, /* 1: time every pass with CUDA events on the handle's stream */
-	TMFQS_OPT_EXACT = 4          /* FP64 handles: 1 (default) bit-identical controlled-phase chains;
+	TMFQS_OPT_EXACT = 4,         /* FP64 handles: 1 (default) bit-identical controlled-phase chains;
 	                                0: each chain as one twiddle per amplitude from FP64 tables
 	                                (about 1e-15 relative error per pass).  FP32 handles always
 	                                use twiddles. */
+	TMFQS_OPT_RADIX = 5          /* fast forms (FP32 handles, or EXACT=0): 1 (default) passes made only
+	                                of Hadamards and controlled phases run as radix-2^k register
+	                                stages; 0: the general fused pass */
 } tmfqs_option;
 
 /* Kernel classes for tmfqs_gpu_kernel_times. */

@@ -103,6 +103,7 @@ class KernelTime(ctypes.Structure):
 KT_NAMES = ("fused", "permute", "gate", "reduce", "grover")
 OPT_KERNEL_TIMING = 3
 OPT_EXACT = 4
+OPT_RADIX = 5
 
 
 class Stats(ctypes.Structure):

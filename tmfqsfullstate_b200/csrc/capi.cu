@@ -293,10 +293,16 @@ struct Planner {
 	std::vector<const tmfqs_op *> pending;  // circuit ops in the pass (for single-op fallback)
 
 	explicit Planner(tmfqs_gpu_state *hh) : h(hh) {
-		const unsigned Kmax = 12;  // 2^12 amplitudes: 64 KB (complex128) / 32 KB (complex64)
-		const unsigned q = h->opt_fused_qubits > 0 ? (unsigned)h->opt_fused_qubits : 9u;
-		mlow = h->precision == TMFQS_FP64 ? 3u : 4u;
-		K = std::min<unsigned>(h->n, std::min<unsigned>(Kmax + (h->precision == TMFQS_FP64 ? 0u : 1u), q + mlow));
+		// Tiles of 2^12 complex128 / 2^13 complex64 amplitudes (64 KB).  The
+		// exact form keeps rows of >= 128 bytes local; the fast forms' radix
+		// passes copy 16-byte granules and take 64-byte rows, which leaves one
+		// more bit per pass for the circuit.
+		const unsigned Kmax = h->precision == TMFQS_FP64 ? 12u : 13u;
+		const bool fast = !h->opt_exact || h->precision == TMFQS_FP32;
+		if(fast && h->opt_radix) mlow = h->precision == TMFQS_FP64 ? 2u : 3u;
+		else mlow = h->precision == TMFQS_FP64 ? 3u : 4u;
+		const unsigned q = h->opt_fused_qubits > 0 ? (unsigned)h->opt_fused_qubits : Kmax - mlow;
+		K = std::min<unsigned>(h->n, std::min<unsigned>(Kmax, q + mlow));
 		reset();
 	}
 
@@ -375,7 +381,9 @@ struct Planner {
 			}
 			pass.gate_count = (unsigned)pending.size();
 			PassTimer timer(h, TMFQS_KT_FUSED, sweep_bytes(h));
-			tqb::launch_fused_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes);
+			const bool done = twiddle && h->opt_radix &&
+			                  tqb::launch_radix_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes);
+			if(!done) tqb::launch_fused_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes);
 			++h->stats.fused_passes;
 		}
 		reset();
@@ -461,6 +469,7 @@ struct Planner {
 				f.mask = (1ull << bc) | (1ull << bt);
 				f.cr = cr;
 				f.ci = ci;
+				f.theta = op.theta;
 				pass.ops.push_back(f);
 				pending.push_back(&op);
 				chain_op = -1;
@@ -786,6 +795,7 @@ int tmfqs_gpu_clone(tmfqs_gpu_state *h, tmfqs_gpu_state **out) {
 			c->opt_fused_qubits = h->opt_fused_qubits;
 			c->opt_grover_fusion = h->opt_grover_fusion;
 			c->opt_exact = h->opt_exact;
+			c->opt_radix = h->opt_radix;
 			if(h->initialized) {
 				flush_dirty(h);
 				ensure_state(c, h->n);
@@ -1281,6 +1291,7 @@ int tmfqs_gpu_set_option(tmfqs_gpu_state *h, int option, long value) {
 			case TMFQS_OPT_GROVER_FUSION: h->opt_grover_fusion = value != 0; break;
 			case TMFQS_OPT_KERNEL_TIMING: h->opt_timing = value != 0; break;
 			case TMFQS_OPT_EXACT: h->opt_exact = value != 0; break;
+			case TMFQS_OPT_RADIX: h->opt_radix = value != 0; break;
 			default: fail(TMFQS_ERR_INVALID_ARGUMENT, "unknown option");
 		}
 	});

@@ -155,20 +155,21 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 							for(unsigned e = 0; e < cnt; ++e) {
 								const double2 ph = cph[e];
 								const int l = cloc[e];
-								R pr0 = (R)ph.x, pi0 = (R)ph.y, pr1 = pr0, pi1 = pi0;
-								if(l >= 0) {
-									// Multiplying by (1, 0) leaves a value unchanged exactly.
-									if(!((j01 >> l) & 1u)) {
-										pr0 = R(1);
-										pi0 = R(0);
-									}
-									if(!((j11 >> l) & 1u)) {
-										pr1 = R(1);
-										pi1 = R(0);
-									}
+								const R pr = (R)ph.x, pi = (R)ph.y;
+								// An entry whose local bit is clear leaves the value as it is
+								// (a product with (1, 0) could turn a -0 component into +0).
+								const bool on0 = l < 0 || ((j01 >> l) & 1u), on1 = l < 0 || ((j11 >> l) & 1u);
+								R s0 = r0, t0 = i0, s1 = r1, t1 = i1;
+								cmul_ref(pr, pi, s0, t0);
+								cmul_ref(pr, pi, s1, t1);
+								if(on0) {
+									r0 = s0;
+									i0 = t0;
 								}
-								cmul_ref(pr0, pi0, r0, i0);
-								cmul_ref(pr1, pi1, r1, i1);
+								if(on1) {
+									r1 = s1;
+									i1 = t1;
+								}
 							}
 							if(c0) {
 								y0.x = r0;

@@ -112,6 +112,7 @@ struct FusedOp {
 	uint64_t mask;   // CNOT: control mask; CP: both bit masks
 	uint64_t state;  // Flip state
 	double cr, ci;   // CP phase
+	double theta;    // CP angle (fast forms)
 };
 
 // One controlled phase of an H-chain, in circuit order (bit positions
@@ -135,6 +136,12 @@ struct FusedPass {
 // Runs one fused pass over the whole state.  `dev_prog` is a device buffer
 // the launcher may (re)use for the program.
 void launch_fused_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, void *&dev_prog,
+                       size_t &dev_prog_bytes);
+
+// Radix-2^RB form of a fused pass for the fast forms (complex64, or complex128
+// without exact arithmetic): programs of H, H-chains, twiddles and controlled
+// phases.  Returns false (nothing launched) when the pass does not qualify.
+bool launch_radix_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, void *&dev_prog,
                        size_t &dev_prog_bytes);
 
 // Involutive permutation of bit positions (disjoint transpositions), as one
@@ -189,7 +196,8 @@ struct tmfqs_gpu_state {
 	bool opt_fusion = true;
 	int opt_fused_qubits = 0;  // 0 = default by precision
 	bool opt_grover_fusion = true;
-	bool opt_exact = true;  // FP64: bit-identical chains (false: one twiddle per |1> output)
+	bool opt_exact = true;
+	bool opt_radix = true;  // fast forms: radix passes where the program allows
 };
 
 #endif
