@@ -299,8 +299,20 @@ struct Planner {
 		// more bit per pass for the circuit.
 		const unsigned Kmax = h->precision == TMFQS_FP64 ? 12u : 13u;
 		const bool fast = !h->opt_exact || h->precision == TMFQS_FP32;
-		if(fast && h->opt_radix) mlow = h->precision == TMFQS_FP64 ? 2u : 3u;
-		else mlow = h->precision == TMFQS_FP64 ? 3u : 4u;
+		if(fast && h->opt_radix) {
+			// Rows of 64 bytes at least; wider rows (up to 256 bytes) stream far
+			// better when the other local bits are high, so take the widest
+			// that still covers all n bits in the fewest passes.
+			const unsigned mmin = h->precision == TMFQS_FP64 ? 2u : 3u, mmax = mmin + 2u;
+			auto passes = [&](unsigned m) -> unsigned {
+				return h->n <= Kmax ? 1u : 1u + (h->n - Kmax + (Kmax - m) - 1u) / (Kmax - m);
+			};
+			mlow = mmin;
+			for(unsigned m = mmin + 1; m <= mmax; ++m)
+				if(passes(m) == passes(mmin)) mlow = m;
+		} else {
+			mlow = h->precision == TMFQS_FP64 ? 3u : 4u;
+		}
 		const unsigned q = h->opt_fused_qubits > 0 ? (unsigned)h->opt_fused_qubits : Kmax - mlow;
 		K = std::min<unsigned>(h->n, std::min<unsigned>(Kmax, q + mlow));
 		reset();

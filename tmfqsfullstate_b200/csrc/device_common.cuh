@@ -51,6 +51,16 @@ __device__ __forceinline__ void cmul_ref(R pr, R pi, R &re, R &im) {
 	im = ni;
 }
 
+// 16-byte asynchronous global -> shared copies (both addresses 16-byte
+// aligned), committed and awaited in groups.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Grid-stride helpers.
 __device__ __forceinline__ uint64_t gtid() { return (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint64_t gstride() { return (uint64_t)gridDim.x * blockDim.x; }

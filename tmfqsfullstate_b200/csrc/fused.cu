@@ -327,16 +327,30 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 // bits are permuted among themselves, so tile o maps to tile perm(o).  A CTA
 // loads tile o and its partner, then writes each to the other's slot with the
 // local bits permuted; tiles fixed by the permutation are permuted alone.
+// Both the permutation of the local index and the shared-memory swizzle are
+// bit-linear, so each is two table lookups (low and high halves of the index).
+// The swizzle XORs the bits that the low bits map to into the low bits: the
+// linear writes and the permuted reads then both spread over the banks.
 // ---------------------------------------------------------------------------
 constexpr unsigned kPermMaxLocal = 12;
+constexpr unsigned kPermThreads = 256;
+constexpr unsigned kPermHalf = 6;  // index bits per lookup table
+constexpr unsigned kPermChunks = 4;  // 6-bit chunks of the tile index (up to 24 outer bits)
+
+// Local bits of a permutation tile: two tiles of 16 KB.
+template <typename R>
+constexpr unsigned perm_max_local() {
+	return sizeof(R) == 8 ? 10u : 11u;
+}
 
 struct PermGeom {
 	unsigned n, K, m;
 	unsigned lpos[kPermMaxLocal];
-	unsigned lmap[kPermMaxLocal];  // local bit i -> local bit lmap[i]
 	unsigned npairs;
 	unsigned pa[32], pb[32];       // all transposed bit-position pairs
 	uint64_t ntiles;
+	uint16_t perm_lo[1 << kPermHalf], perm_hi[1 << kPermHalf];  // local index permutation
+	uint16_t swz_lo[1 << kPermHalf], swz_hi[1 << kPermHalf];    // shared-memory swizzle (XOR)
 };
 
 __device__ __forceinline__ uint64_t perm_global(uint64_t x, const PermGeom &g) {
@@ -357,49 +371,110 @@ __device__ __forceinline__ uint64_t compress_outer(uint64_t x, const PermGeom &g
 	return x;
 }
 
-__device__ __forceinline__ unsigned perm_local(unsigned j, const PermGeom &g) {
-	unsigned r = 0;
-	for(unsigned i = 0; i < g.K; ++i)
-		if((j >> i) & 1u) r |= 1u << g.lmap[i];
-	return r;
-}
-
 template <typename R>
-__global__ void __launch_bounds__(256) k_bit_perm(typename Vec2<R>::type *a, PermGeom g) {
+__global__ void __launch_bounds__(kPermThreads) k_bit_perm(typename Vec2<R>::type *a, PermGeom g) {
 	typedef typename Vec2<R>::type V;
-	extern __shared__ unsigned char smem_raw[];
+	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const unsigned T = 1u << g.K;
-	V *A = reinterpret_cast<V *>(smem_raw);
-	V *B = A + T;
-	uint64_t *hitab = reinterpret_cast<uint64_t *>(B + T);
-	const unsigned nhi = 1u << (g.K - g.m);
+	// Two buffers, each the tile and its partner; the next pair's copies are in
+	// flight while the current pair is written out.
+	V *buf = reinterpret_cast<V *>(smem_raw);
+	uint64_t *hitab = reinterpret_cast<uint64_t *>(buf + 4 * T);
+	// Tile o -> (its base, the partner's base, the partner's tile index): all
+	// three maps are bit-linear, so they are ORs of per-chunk table entries.
+	uint64_t *otab = hitab + (1u << (g.K - g.m));  // [kPermChunks][64][3]
+	uint16_t *tabs = reinterpret_cast<uint16_t *>(otab + kPermChunks * 64 * 3);
+	const unsigned nhi = 1u << (g.K - g.m), H = 1u << kPermHalf, hm = H - 1u;
+	for(unsigned e = threadIdx.x; e < kPermChunks * 64; e += blockDim.x) {
+		uint64_t base = (uint64_t)(e & 63u) << (6u * (e >> 6));
+		for(unsigned i = 0; i < g.K; ++i) base = insert0(base, g.lpos[i]);
+		const uint64_t pbase = perm_global(base, g);
+		otab[3 * e] = base;
+		otab[3 * e + 1] = pbase;
+		otab[3 * e + 2] = compress_outer(pbase, g);
+	}
 	for(unsigned h = threadIdx.x; h < nhi; h += blockDim.x) {
 		uint64_t v = 0;
 		for(unsigned i = 0; i < g.K - g.m; ++i)
 			if((h >> i) & 1u) v |= 1ull << g.lpos[g.m + i];
 		hitab[h] = v;
 	}
+	for(unsigned k = threadIdx.x; k < H; k += blockDim.x) {
+		tabs[k] = g.perm_lo[k];
+		tabs[H + k] = g.perm_hi[k];
+		tabs[2 * H + k] = g.swz_lo[k];
+		tabs[3 * H + k] = g.swz_hi[k];
+	}
 	__syncthreads();
 	const unsigned lowmask = (1u << g.m) - 1u;
 	auto scatter = [&](unsigned j) -> uint64_t { return (uint64_t)(j & lowmask) | hitab[j >> g.m]; };
-	for(uint64_t o = blockIdx.x; o < g.ntiles; o += gridDim.x) {
-		uint64_t base = o;
-		for(unsigned i = 0; i < g.K; ++i) base = insert0(base, g.lpos[i]);
-		const uint64_t pbase = perm_global(base, g);
-		const uint64_t po = compress_outer(pbase, g);
-		if(po < o) continue;  // handled with its partner
-		for(unsigned j = threadIdx.x; j < T; j += blockDim.x) A[j] = a[base | scatter(j)];
-		if(po != o)
-			for(unsigned j = threadIdx.x; j < T; j += blockDim.x) B[j] = a[pbase | scatter(j)];
+	auto perm = [&](unsigned j) -> unsigned { return (unsigned)tabs[j & hm] | tabs[H + (j >> kPermHalf)]; };
+	auto phys = [&](unsigned j) -> unsigned { return j ^ tabs[2 * H + (j & hm)] ^ tabs[3 * H + (j >> kPermHalf)]; };
+	struct Work {
+		uint64_t o, base, pbase, po;
+	};
+	auto work_at = [&](uint64_t o) -> Work {
+		Work w{o, 0, 0, 0};
+#pragma unroll
+		for(unsigned c = 0; c < kPermChunks; ++c) {
+			const uint64_t *t = otab + 3 * ((c << 6) | (unsigned)((o >> (6u * c)) & 63u));
+			w.base |= t[0];
+			w.pbase |= t[1];
+			w.po |= t[2];
+		}
+		return w;
+	};
+	// The first tile of this CTA at or after o whose partner is not smaller
+	// (a pair is handled once, by its smaller tile).
+	auto next_work = [&](uint64_t o) -> Work {
+		for(; o < g.ntiles; o += gridDim.x) {
+			const Work w = work_at(o);
+			if(w.po >= w.o) return w;
+		}
+		return Work{g.ntiles, 0, 0, 0};
+	};
+	// Global memory moves in 16-byte granules of G consecutive amplitudes
+	// (local bit 0 is global bit 0).  The swizzle keeps granules whole.
+	constexpr unsigned G = 16 / sizeof(V);
+	const unsigned TG = T / G;
+	auto prefetch = [&](const Work &w, V *dst) {
+		if(w.o < g.ntiles) {
+			for(unsigned q = threadIdx.x; q < TG; q += blockDim.x) {
+				const unsigned j = q * G;
+				cp_async16(dst + phys(j), a + (w.base | scatter(j)));
+				if(w.po != w.o) cp_async16(dst + T + phys(j), a + (w.pbase | scatter(j)));
+			}
+		}
+		cp_async_commit();
+	};
+	Work cur = next_work(blockIdx.x);
+	unsigned sel = 0;
+	prefetch(cur, buf);
+	while(cur.o < g.ntiles) {
+		const Work nxt = next_work(cur.o + gridDim.x);
+		prefetch(nxt, buf + 2 * T * (sel ^ 1u));
+		cp_async_wait1();
 		__syncthreads();
-		// amplitude (base|scatter(j)) moves to (pbase|scatter(perm_local(j))).
-		for(unsigned jw = threadIdx.x; jw < T; jw += blockDim.x) {
-			const unsigned js = perm_local(jw, g);  // involution: source of slot jw
-			a[pbase | scatter(jw)] = A[js];
-			if(po != o) a[base | scatter(jw)] = B[js];
+		const V *A = buf + 2 * T * sel, *B = A + T;
+		const bool pair = cur.po != cur.o;
+		// amplitude (base|scatter(j)) moves to (pbase|scatter(perm(j))).
+		for(unsigned q = threadIdx.x; q < TG; q += blockDim.x) {
+			float4 wa, wb;
+			V *ya = reinterpret_cast<V *>(&wa), *yb = reinterpret_cast<V *>(&wb);
+#pragma unroll
+			for(unsigned e = 0; e < G; ++e) {
+				const unsigned js = phys(perm(q * G + e));  // involution: source of slot q*G+e
+				ya[e] = A[js];
+				if(pair) yb[e] = B[js];
+			}
+			*reinterpret_cast<float4 *>(a + (cur.pbase | scatter(q * G))) = wa;
+			if(pair) *reinterpret_cast<float4 *>(a + (cur.base | scatter(q * G))) = wb;
 		}
 		__syncthreads();
+		cur = nxt;
+		sel ^= 1u;
 	}
+	cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -520,7 +595,7 @@ void run_perm(const LaunchCtx &c, void *a, unsigned n, const std::vector<std::pa
 		img[pairs[i].first] = (int)pairs[i].second;
 		img[pairs[i].second] = (int)pairs[i].first;
 	}
-	const unsigned maxK = sizeof(R) == 8 ? 10u : 11u;  // two tiles of 16/32 KB
+	const unsigned maxK = perm_max_local<R>();
 	// Grow the low run r while the closed local set fits.
 	std::vector<unsigned> best;
 	for(unsigned r = 1; r <= n; ++r) {
@@ -538,18 +613,48 @@ void run_perm(const LaunchCtx &c, void *a, unsigned n, const std::vector<std::pa
 	g.K = (unsigned)best.size();
 	g.m = 0;
 	while(g.m < g.K && best[g.m] == g.m) ++g.m;
+	if(g.m < 1) fail(TMFQS_ERR_LOGIC, "bit permutation: bit 0 must be local");
+	std::vector<unsigned> lmap(g.K);
 	for(unsigned i = 0; i < g.K; ++i) {
 		g.lpos[i] = best[i];
 		const unsigned target = (unsigned)img[best[i]];
-		g.lmap[i] = (unsigned)(std::find(best.begin(), best.end(), target) - best.begin());
+		lmap[i] = (unsigned)(std::find(best.begin(), best.end(), target) - best.begin());
+	}
+	// Swizzled bits: the 16-byte granule index within 128 bytes (bits s0 to
+	// s0+2 of the local index), so copies of whole granules stay contiguous.
+	const unsigned s0 = sizeof(R) == 8 ? 0u : 1u, b = std::min<unsigned>(g.K, s0 + 3u);
+	auto perm_of = [&](unsigned j) {
+		unsigned r = 0;
+		for(unsigned i = 0; i < g.K; ++i)
+			if((j >> i) & 1u) r |= 1u << lmap[i];
+		return r;
+	};
+	// swizzle(j): for each bit s0 <= i < b whose image lmap[i] is at or above
+	// b, the bit of j at lmap[i] is XORed into bit i.
+	auto swz_of = [&](unsigned j) {
+		unsigned x = 0;
+		for(unsigned i = s0; i < b; ++i)
+			if(lmap[i] >= b && ((j >> lmap[i]) & 1u)) x |= 1u << i;
+		return x;
+	};
+	const unsigned H = 1u << kPermHalf;
+	for(unsigned k = 0; k < H; ++k) {
+		const unsigned lo = k < (1u << std::min(g.K, kPermHalf)) ? k : 0u;
+		const unsigned hi = g.K > kPermHalf && k < (1u << (g.K - kPermHalf)) ? (k << kPermHalf) : 0u;
+		g.perm_lo[k] = (uint16_t)perm_of(lo);
+		g.perm_hi[k] = (uint16_t)perm_of(hi);
+		g.swz_lo[k] = (uint16_t)swz_of(lo);
+		g.swz_hi[k] = (uint16_t)swz_of(hi);
 	}
 	g.ntiles = 1ull << (n - g.K);
-	const size_t smem = 2 * (sizeof(typename Vec2<R>::type) << g.K) + (sizeof(uint64_t) << (g.K - g.m));
+	if(n - g.K > 6 * kPermChunks) fail(TMFQS_ERR_INVALID_ARGUMENT, "bit permutation: state too large");
+	const size_t smem = 4 * (sizeof(typename Vec2<R>::type) << g.K) + (sizeof(uint64_t) << (g.K - g.m)) +
+	                    sizeof(uint64_t) * kPermChunks * 64 * 3 + 4 * H * sizeof(uint16_t);
 	check_cuda(cudaFuncSetAttribute(k_bit_perm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "perm smem");
 	int per_sm = 1;
-	check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bit_perm<R>, 256, smem), "perm occupancy");
+	check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bit_perm<R>, kPermThreads, smem), "perm occupancy");
 	const uint64_t grid = std::min<uint64_t>(g.ntiles, (uint64_t)c.num_sms * std::max(1, per_sm));
-	k_bit_perm<R><<<(unsigned)grid, 256, smem, c.stream>>>(static_cast<typename Vec2<R>::type *>(a), g);
+	k_bit_perm<R><<<(unsigned)grid, kPermThreads, smem, c.stream>>>(static_cast<typename Vec2<R>::type *>(a), g);
 	after_launch(c, "bit permutation");
 }
 

@@ -47,7 +47,15 @@ constexpr unsigned kRadixMaxSlots = 48;
 //   kRIButterflyTw  butterflies, then the |1> outputs times a 2^(RB-1)-entry
 //                   table (the in-stage phases that follow a Hadamard)
 //   kRIDiag         every register times a 2^RB-entry table
-enum RadixItemKind : uint32_t { kRIButterfly = 0, kRIButterflyTw = 1, kRIDiag = 2 };
+//   kRIQft          the QFT ladder on register bits 0..d-1 (d in bits 8-15):
+//                   Hadamards in bit order, and after the one on bit i the
+//                   controlled phases pi/2^(j-i) with every later bit j, as a
+//                   compiled butterfly network with the roots of unity below
+enum RadixItemKind : uint32_t { kRIButterfly = 0, kRIButterflyTw = 1, kRIDiag = 2, kRIQft = 3 };
+
+// cos and sin of 2*pi*k/32, k < 16 (host C library, FP64): the twiddles of
+// the compiled QFT stages.
+constexpr unsigned kRoots = 16;
 
 struct RadixStage {
 	uint32_t first, count;    // items of the stage
@@ -79,7 +87,13 @@ struct RadixGeom {
 	unsigned lpos[14];          // ascending local bit positions
 	uint64_t ntiles;
 	unsigned nstages, nitems, ntab, nslots, nterms;
+	double root[kRoots][2];     // FP64 roots (complex128 states)
+	float rootf[kRoots][2];     // the same rounded once (complex64 states)
 };
+
+// Root k as a storage-type value, read from the kernel parameters.
+__device__ __forceinline__ void root_of(const RadixGeom &g, int k, double2 &r) { r = make_double2(g.root[k][0], g.root[k][1]); }
+__device__ __forceinline__ void root_of(const RadixGeom &g, int k, float2 &r) { r = make_float2(g.rootf[k][0], g.rootf[k][1]); }
 
 template <typename V>
 struct RadixSmem {
@@ -122,12 +136,6 @@ __device__ __forceinline__ V vmul(V a, V b) {
 	return r;
 }
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 __device__ __forceinline__ unsigned rinsert0(unsigned x, unsigned b) {
 	const unsigned lo = x & ((1u << b) - 1u);
@@ -156,6 +164,19 @@ __device__ __forceinline__ float2 to_v<float2>(double2 d) {
 	return make_float2((float)d.x, (float)d.y);
 }
 
+// One unscaled butterfly: (x, y) <- (x + y, x - y).  Complex64 values use
+// the paired FP32 instructions (one instruction per complex add).
+__device__ __forceinline__ void bfly2(double2 &x, double2 &y) {
+	const double2 a = x, b = y;
+	x = make_double2(a.x + b.x, a.y + b.y);
+	y = make_double2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ void bfly2(float2 &x, float2 &y) {
+	const float2 a = x, b = y;
+	x = __fadd2_rn(a, b);
+	y = __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+
 // Butterflies on register bit TB (unscaled); with `tw`, the |1> output of
 // pair q is then multiplied by tw[q].
 template <typename V, int RB, int TB>
@@ -164,11 +185,7 @@ __device__ __forceinline__ void rbfly(V (&v)[1 << RB], const V *tw) {
 #pragma unroll
 	for(int q = 0; q < (1 << (RB - 1)); ++q) {
 		const int r0 = ((q & ~lo) << 1) | (q & lo), r1 = r0 | (1 << TB);
-		const V x = v[r0], y = v[r1];
-		v[r0].x = x.x + y.x;
-		v[r0].y = x.y + y.y;
-		v[r1].x = x.x - y.x;
-		v[r1].y = x.y - y.y;
+		bfly2(v[r0], v[r1]);
 	}
 	if(tw) {
 #pragma unroll
@@ -187,6 +204,81 @@ __device__ __forceinline__ void rbfly_dispatch(V (&v)[1 << RB], unsigned b, cons
 		case 2: if constexpr(RB > 2) rbfly<V, RB, 2>(v, tw); break;
 		case 3: if constexpr(RB > 3) rbfly<V, RB, 3>(v, tw); break;
 		case 4: if constexpr(RB > 4) rbfly<V, RB, 4>(v, tw); break;
+		default: break;
+	}
+}
+
+// v times exp(2*pi*i*k/32), k < 16 known at compile time: exact for k = 0 and
+// k = 8 (the factor i), otherwise a complex product with the tabulated root.
+template <int k, typename V>
+__device__ __forceinline__ V mul_root(V v, const RadixGeom &g) {
+	if constexpr(k == 0) {
+		return v;
+	} else if constexpr(k == 8) {
+		V r;
+		r.x = -v.y;
+		r.y = v.x;
+		return r;
+	} else {
+		V w;
+		root_of(g, k, w);
+		return vmul(v, w);
+	}
+}
+
+// The QFT ladder on register bits 0..D-1.  After the butterflies on bit i,
+// the |1> output at register r gets exp(2*pi*i*K/2^(D-i)) with
+// K = sum_{j>i} r_j 2^(D-1-j): the phases pi/2^(j-i) of the controlled phases
+// between bit i and each later bit j.
+template <typename V, int RB, int D>
+__device__ __forceinline__ void qft_stage(V (&v)[1 << RB], const RadixGeom &g) {
+#pragma unroll
+	for(int i = 0; i < D; ++i) {
+#pragma unroll
+		for(int q = 0; q < (1 << (RB - 1)); ++q) {
+			const int lo = (1 << i) - 1;
+			const int r0 = ((q & ~lo) << 1) | (q & lo), r1 = r0 | (1 << i);
+			bfly2(v[r0], v[r1]);
+		}
+#pragma unroll
+		for(int r = 0; r < (1 << RB); ++r) {
+			if(!((r >> i) & 1)) continue;
+			int K = 0;
+#pragma unroll
+			for(int j = i + 1; j < D; ++j) K |= ((r >> j) & 1) << (D - 1 - j);
+			// exp(2 pi i K / 2^(D-i)) = root[K * 32 / 2^(D-i)]
+			const int idx = K << (5 - (D - i));
+			switch(idx) {
+				case 0: break;
+				case 1: v[r] = mul_root<1>(v[r], g); break;
+				case 2: v[r] = mul_root<2>(v[r], g); break;
+				case 3: v[r] = mul_root<3>(v[r], g); break;
+				case 4: v[r] = mul_root<4>(v[r], g); break;
+				case 5: v[r] = mul_root<5>(v[r], g); break;
+				case 6: v[r] = mul_root<6>(v[r], g); break;
+				case 7: v[r] = mul_root<7>(v[r], g); break;
+				case 8: v[r] = mul_root<8>(v[r], g); break;
+				case 9: v[r] = mul_root<9>(v[r], g); break;
+				case 10: v[r] = mul_root<10>(v[r], g); break;
+				case 11: v[r] = mul_root<11>(v[r], g); break;
+				case 12: v[r] = mul_root<12>(v[r], g); break;
+				case 13: v[r] = mul_root<13>(v[r], g); break;
+				case 14: v[r] = mul_root<14>(v[r], g); break;
+				case 15: v[r] = mul_root<15>(v[r], g); break;
+				default: break;
+			}
+		}
+	}
+}
+
+template <typename V, int RB>
+__device__ __forceinline__ void qft_dispatch(V (&v)[1 << RB], unsigned d, const RadixGeom &g) {
+	switch(d) {
+		case 1: qft_stage<V, RB, 1>(v, g); break;
+		case 2: if constexpr(RB >= 2) qft_stage<V, RB, 2>(v, g); break;
+		case 3: if constexpr(RB >= 3) qft_stage<V, RB, 3>(v, g); break;
+		case 4: if constexpr(RB >= 4) qft_stage<V, RB, 4>(v, g); break;
+		case 5: if constexpr(RB >= 5) qft_stage<V, RB, 5>(v, g); break;
 		default: break;
 	}
 }
@@ -364,7 +456,9 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 				const uint32_t it = sh.items[k];
 				const unsigned kind = it & 0xffu, b = (it >> 8) & 0xffu;
 				const V *tb = sh.tabs + (it >> 16);
-				if(kind == kRIDiag) {
+				if(kind == kRIQft) {
+					qft_dispatch<V, RB>(v, b, g);
+				} else if(kind == kRIDiag) {
 #pragma unroll
 					for(int r = 0; r < (1 << RB); ++r) v[r] = vmul(v[r], tb[r]);
 				} else {
@@ -411,7 +505,7 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 		__syncthreads();
 	}
 	// Drain the (empty) groups committed past the last tile.
-	asm volatile("cp.async.wait_all;\n" ::: "memory");
+	cp_async_wait_all();
 }
 
 }  // namespace
@@ -458,6 +552,13 @@ bool build_radix_program(const FusedPass &pass, unsigned K, size_t vbytes, Radix
 	while(g.m < K && pass.lpos[g.m] == g.m) ++g.m;
 	g.ntiles = 1ull << (pass.n - K);
 	g.lo = (K + 1) / 2;
+	const double two_pi = 2.0 * std::acos(-1.0);
+	for(unsigned k = 0; k < kRoots; ++k) {
+		g.root[k][0] = std::cos(two_pi * k / 32.0);
+		g.root[k][1] = std::sin(two_pi * k / 32.0);
+		g.rootf[k][0] = (float)g.root[k][0];
+		g.rootf[k][1] = (float)g.root[k][1];
+	}
 	auto ref_of = [&](unsigned bit) -> BitRef {
 		for(unsigned i = 0; i < K; ++i)
 			if(pass.lpos[i] == bit) return BitRef{true, i};
@@ -566,19 +667,21 @@ bool build_radix_program(const FusedPass &pass, unsigned K, size_t vbytes, Radix
 			last_bfly = -1;
 			run.clear();
 		};
+		// The stage as (Hadamard register bit, in-stage phases that follow it);
+		// phases before the first Hadamard have register bit -1.
+		std::vector<std::pair<int, std::vector<const PItem *>>> seq;
 		std::vector<unsigned> hseen;
 		for(size_t k : s.items) {
 			const PItem &it = items[k];
 			if(it.is_h) {
-				flush_run();
-				last_bfly = regidx(BitRef{true, it.l});
-				P.items.push_back(kRIButterfly | ((uint32_t)last_bfly << 8));
+				seq.push_back({regidx(BitRef{true, it.l}), {}});
 				hseen.push_back(it.l);
 				continue;
 			}
 			const int ra = regidx(it.b0), rc = regidx(it.b1);
 			if(ra >= 0 && rc >= 0) {
-				run.push_back(&it);
+				if(seq.empty()) seq.push_back({-1, {}});
+				seq.back().second.push_back(&it);
 				continue;
 			}
 			if(ra < 0 && rc < 0) {
@@ -594,7 +697,40 @@ bool build_radix_program(const FusedPass &pass, unsigned K, size_t vbytes, Radix
 			// stage start; after it (or with none): moved to the stage end.
 			(h_before || !has_h ? post : pre)[reg + 1].push_back(STerm{other, {}, false, it.theta});
 		}
-		flush_run();
+		// The QFT ladder: Hadamard i (register bit i, in order) followed by the
+		// controlled phases pi/2^(j-i) with every later Hadamard bit j.
+		const int d = (int)s.hbits.size();
+		bool qft = (int)seq.size() == d;
+		for(int i = 0; qft && i < d; ++i) {
+			const auto &T = seq[i].second;
+			if(seq[i].first != i || (int)T.size() != d - 1 - i) {
+				qft = false;
+				break;
+			}
+			uint32_t seen = 0;
+			for(const PItem *t : T) {
+				const int a = regidx(t->b0), c = regidx(t->b1);
+				const int other = a == i ? c : (c == i ? a : -1);
+				const double want = std::ldexp(std::acos(-1.0), -(other - i));
+				if(other <= i || other >= d || ((seen >> other) & 1u) || std::fabs(t->theta - want) > 1e-12 * want) {
+					qft = false;
+					break;
+				}
+				seen |= 1u << other;
+			}
+		}
+		if(qft) {
+			P.items.push_back(kRIQft | ((uint32_t)d << 8));
+		} else {
+			for(auto &e : seq) {
+				if(e.first >= 0) {
+					P.items.push_back(kRIButterfly | ((uint32_t)e.first << 8));
+					last_bfly = e.first;
+				}
+				run = e.second;
+				flush_run();
+			}
+		}
 		S.count = (uint32_t)P.items.size() - S.first;
 
 		const bool last = si + 1 == st.size();
