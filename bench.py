@@ -15,6 +15,11 @@ between steps.
   e2e     the same metric through the C ABI with host buffers: each step
           loads the input from pinned host memory, runs the QFT, and reads
           back the exact total probability and a seeded measurement.
+  forms   the same QFT in the two fast forms on the same GPU, device-resident:
+          complex64 (radix passes, FP64 twiddles rounded once) and complex128
+          with TMFQS_OPT_EXACT=0; each with its amp-updates/s, the HBM
+          fraction of its passes, and its accuracy against the plain result
+          (relative L2 error, fidelity, measured index).
   --impl reference   the reference's own Dense CPU path (oracle/_ref, compiled
           from the reference sources) on this host, on a bounded prefix of the
           same circuit.
@@ -45,12 +50,14 @@ REF_PREFIX_OPS = 8  # reference CPU sample: H(0) + 7 controlled phases of QFT-28
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=25)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--qubits", type=int, default=28)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--form-steps", type=int, default=3)
+    p.add_argument("--no-forms", action="store_true")
     return p.parse_args()
 
 
@@ -115,6 +122,13 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        # Wait (up to 10 s) for the first sample so the timed region is covered.
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -144,6 +158,60 @@ class ClockSampler:
         load = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
         return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def pass_roofline(kt, name, peak):
+    k = kt[name]
+    if not k["launches"]:
+        return None
+    bytes_per = k["bytes"] / k["launches"]
+    avg_ms = k["ms"] / k["launches"]
+    achieved = bytes_per / (avg_ms / 1e3) / 1e9
+    return {"launches": k["launches"], "bytes_per_launch": bytes_per, "avg_launch_ms": avg_ms,
+            "achieved_gbs": achieved, "frac": achieved / peak}
+
+
+def run_form(tq, torch, n, inp, ops, prec, exact, steps, peak, plain, rnd, device):
+    """One fast form of the QFT on the same input: device-resident timing and accuracy."""
+    import numpy as np
+
+    g = tq.GpuState(prec, device)
+    g.set_option(tq.OPT_EXACT, 1 if exact else 0)
+    stream = torch.cuda.ExternalStream(g.stream())
+    g.load(n, inp)
+    g.apply_ops(ops)  # warm-up
+    ms = []
+    kts = []
+    for _ in range(steps):
+        g.load(n, inp)
+        g.sync()
+        g.reset_stats()
+        g.set_option(tq.OPT_KERNEL_TIMING, 1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.apply_ops(ops)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        kts.append(g.kernel_times())
+        g.set_option(tq.OPT_KERNEL_TIMING, 0)
+    best = min(range(steps), key=lambda i: ms[i])
+    kt = kts[best]
+    t = ms[best]
+    got = g.export()
+    measured = g.sample(rnd)
+    g.close()
+    ca = plain[0::2] + 1j * plain[1::2]
+    cb = got[0::2] + 1j * got[1::2]
+    fid = abs(np.vdot(ca, cb)) ** 2 / (np.vdot(ca, ca).real * np.vdot(cb, cb).real)
+    rel = float(np.linalg.norm(plain - got) / np.linalg.norm(plain))
+    sweep = 2 * (8 if prec == tq.FP32 else 16) * (1 << n)
+    passes = kt["fused"]["launches"] + kt["permute"]["launches"]
+    return {"ms_per_qft": t, "value": len(ops) * (1 << n) / (t / 1e3), "unit": UNIT,
+            "hbm_frac_whole_qft": passes * sweep / (t / 1e3) / 1e9 / peak,
+            "sweeps": passes, "fused_pass": pass_roofline(kt, "fused", peak),
+            "permute_pass": pass_roofline(kt, "permute", peak),
+            "rel_l2_vs_plain": rel, "fidelity_vs_plain": float(fid), "measured": measured}
 
 
 def run_ours(args):
@@ -236,6 +304,16 @@ def run_ours(args):
                     "traffic": profiled_traffic(n), "bytes_per_launch": bytes_per, "avg_launch_ms": avg_ms,
                     "share_of_step": fused["ms"] / ms if ms else None}
 
+    forms = None
+    if rank == 0 and not args.no_forms:
+        plain = g.export()
+        forms = {}
+        for name, prec, exact in (("complex64_radix", tq.FP32, True), ("complex128_fast", tq.FP64, False)):
+            forms[name] = run_form(tq, torch, n, inp, ops, prec, exact, max(1, args.form_steps), peak, plain, rnd,
+                                   local)
+            forms[name]["speedup_vs_plain"] = (ms_per_step / forms[name]["ms_per_qft"])
+        del plain
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(n)
@@ -250,7 +328,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16 * N, "d2h_bytes_per_step": 16,
                     "ms_per_step": e2e_s * 1e3},
             "gpu_launches": int(stats["kernel_launches"]),
-            "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "forms": forms,
             "kernel_times_ms": {k: round(v["ms"], 3) for k, v in kt.items() if v["launches"]},
             "check": {"total_probability": total, "measured": measured,
                       "reference_golden": {"total_probability": 0.99999999999986022, "measured": 138222191}},
