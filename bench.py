@@ -20,6 +20,12 @@ between steps.
           with TMFQS_OPT_EXACT=0; each with its amp-updates/s, the HBM
           fraction of its passes, and its accuracy against the plain result
           (relative L2 error, fidelity, measured index).
+  adjoint the differentiation form (24 qubits, 20 layers of H + ring
+          controlled phases, 480 angles, E = sum_q <Z_q Z_{q+1}>): complex64
+          forward and adjoint backward with a checkpoint every 48 ops; grad/s,
+          backward/forward cost, and the error against the reference's
+          parameter-shift gradients (tests/golden/adjoint_ps_n24.json) and
+          FP64 central finite differences on the same 32 angles.
   --impl reference   the reference's own Dense CPU path (oracle/_ref, compiled
           from the reference sources) on this host, on a bounded prefix of the
           same circuit.
@@ -58,6 +64,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--form-steps", type=int, default=3)
     p.add_argument("--no-forms", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
     return p.parse_args()
 
 
@@ -214,6 +221,60 @@ def run_form(tq, torch, n, inp, ops, prec, exact, steps, peak, plain, rnd, devic
             "rel_l2_vs_plain": rel, "fidelity_vs_plain": float(fid), "measured": measured}
 
 
+def run_adjoint(tq, torch, device, reps=3):
+    """Configuration 5: the adjoint gradient in complex64 and its checks."""
+    import numpy as np
+
+    n, layers, every = 24, 20, 48
+    th = tq.random_angles(n * layers, SEED)
+    ops = tq.layered_cphase_ops(n, th)
+    masks, weights = tq.zz_ring_observable(n)
+    g = tq.GpuState(tq.FP32, device)
+    g.init_basis(n, 0)
+    g.apply_ops(ops)  # warm-up
+    g.adjoint_gradient(ops, masks, weights, every)
+    fwd, tot = [], []
+    for _ in range(reps):
+        g.init_basis(n, 0)
+        g.sync()
+        t0 = time.perf_counter()
+        g.apply_ops(ops)
+        fwd.append(time.perf_counter() - t0)
+        g.init_basis(n, 0)
+        g.sync()
+        t0 = time.perf_counter()
+        e, grads = g.adjoint_gradient(ops, masks, weights, every)
+        tot.append(time.perf_counter() - t0)
+    g.close()
+    f, t = min(fwd), min(tot)
+    out = {"n_qubits": n, "layers": layers, "angles": len(grads), "form": "complex64", "checkpoint_every": every,
+           "forward_ms": f * 1e3, "forward_backward_ms": t * 1e3, "backward_over_forward": (t - f) / f,
+           "grad_per_s": len(grads) / t, "expectation": e}
+    gold_path = os.path.join(ROOT, "tests", "golden", "adjoint_ps_n24.json")
+    if os.path.exists(gold_path):
+        with open(gold_path) as fh:
+            gold = json.load(fh)
+        idx = gold["indices"]
+        out["max_abs_err_vs_reference_parameter_shift"] = float(np.max(np.abs(grads[idx] - np.array(gold["ps_grad"]))))
+        out["expectation_err_vs_reference"] = abs(e - gold["expectation"])
+        # FP64 central differences (h = 1e-6) on the same angles, complex128 fast form on the GPU.
+        h = tq.GpuState(tq.FP64, device)
+        h.set_option(tq.OPT_EXACT, 0)
+        fd = []
+        for i in idx:
+            es = []
+            for s in (+1e-6, -1e-6):
+                tt = th.copy()
+                tt[i] += s
+                h.init_basis(n, 0)
+                es.append(h.adjoint_gradient(tq.layered_cphase_ops(n, tt), masks, weights, 0)[0])
+            fd.append((es[0] - es[1]) / 2e-6)
+        h.close()
+        out["max_abs_err_vs_fp64_fd"] = float(np.max(np.abs(grads[idx] - np.array(fd))))
+        out["checked_angles"] = len(idx)
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -314,6 +375,10 @@ def run_ours(args):
             forms[name]["speedup_vs_plain"] = (ms_per_step / forms[name]["ms_per_qft"])
         del plain
 
+    adjoint = None
+    if rank == 0 and not args.no_adjoint:
+        adjoint = run_adjoint(tq, torch, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(n)
@@ -329,6 +394,7 @@ def run_ours(args):
                     "ms_per_step": e2e_s * 1e3},
             "gpu_launches": int(stats["kernel_launches"]),
             "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "forms": forms,
+            "adjoint": adjoint,
             "kernel_times_ms": {k: round(v["ms"], 3) for k, v in kt.items() if v["launches"]},
             "check": {"total_probability": total, "measured": measured,
                       "reference_golden": {"total_probability": 0.99999999999986022, "measured": 138222191}},

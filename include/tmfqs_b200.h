@@ -120,7 +120,8 @@ typedef enum {
 	TMFQS_KT_GATE = 2,    /* single-gate pass (incl. diffusion and affine sweeps) */
 	TMFQS_KT_REDUCE = 3,  /* exact reduction (sum, norm, measurement) */
 	TMFQS_KT_GROVER = 4,  /* temporal Grover pass */
-	TMFQS_KT_COUNT = 5
+	TMFQS_KT_ADJOINT = 5, /* adjoint-gradient passes (observable, gradient runs) */
+	TMFQS_KT_COUNT = 6
 } tmfqs_kernel_class;
 
 /* Accumulated device time of one kernel class since the last reset:
@@ -233,6 +234,25 @@ TMFQS_API int tmfqs_gpu_grover_run(tmfqs_gpu_state *h, tmfqs_register_view *view
  * and each call returns after the result is on the host. */
 TMFQS_API int tmfqs_sample_static(const void *device_amps, int precision, unsigned num_qubits, double rnd,
                                   void *stream, uint64_t *index_out);
+/* The differentiation form (no reference counterpart; its checks use the
+ * reference's Dense forward through the parameter-shift rule).  Runs `ops` on
+ * the handle's current state psi_0 (the forward pass: the same fused passes as
+ * tmfqs_gpu_apply_ops), and returns the expectation E = <psi|O|psi> of the
+ * diagonal observable O = sum_j obs_weights[j] * Z(obs_masks[j]) -- Z(m) is the
+ * product of Pauli Z over the qubits whose index bits are set in m (qubit q is
+ * bit n-1-q), eigenvalue (-1)^popcount(x & m) -- and dE/dtheta for every
+ * TMFQS_OP_CPHASE in `ops`, in op order, in `grads` (one double each).
+ * Reverse-mode: lambda = O psi is carried back through the inverse circuit;
+ * each run of consecutive diagonal ops (controlled phases, phase flips) gets
+ * all its derivatives from one read of lambda and psi.  psi is checkpointed
+ * every `checkpoint_every` ops of the forward pass (0: the smallest interval
+ * whose checkpoints fit in half the free device memory) and restored from the
+ * checkpoints in the backward pass, which bounds the complex64 drift of psi.
+ * Ops: H, X, CNOT, CPHASE, SWAP, PHASE_FLIP, GATE (INVERSION is rejected);
+ * 1 <= obs_terms <= 64.  On return the handle holds the final state. */
+TMFQS_API int tmfqs_gpu_adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count,
+                                         const uint64_t *obs_masks, const double *obs_weights, unsigned obs_terms,
+                                         size_t checkpoint_every, double *expectation, double *grads);
 /* endOperationBatch, i_state_backend.h:163: waits for all queued work. */
 TMFQS_API int tmfqs_gpu_sync(tmfqs_gpu_state *h);
 

@@ -100,7 +100,7 @@ class KernelTime(ctypes.Structure):
     _fields_ = [("launches", ctypes.c_uint64), ("ms", ctypes.c_double), ("bytes", ctypes.c_double)]
 
 
-KT_NAMES = ("fused", "permute", "gate", "reduce", "grover")
+KT_NAMES = ("fused", "permute", "gate", "reduce", "grover", "adjoint")
 OPT_KERNEL_TIMING = 3
 OPT_EXACT = 4
 OPT_RADIX = 5
@@ -158,6 +158,8 @@ SIGNATURES = {
     "tmfqs_gpu_swap": [_H, _UI, _UI],
     "tmfqs_gpu_apply_ops": [_H, ctypes.POINTER(Op), ctypes.c_size_t],
     "tmfqs_gpu_grover_run": [_H, ctypes.POINTER(RegisterView), _U64P, ctypes.c_size_t, _U64, ctypes.c_int],
+    "tmfqs_gpu_adjoint_gradient": [_H, ctypes.POINTER(Op), ctypes.c_size_t, _U64P, _DP, _UI, ctypes.c_size_t, _DP,
+                                   _DP],
     "tmfqs_gpu_sync": [_H],
     "tmfqs_gpu_stats": [_H, ctypes.POINTER(Stats)],
     "tmfqs_gpu_reset_stats": [_H],
@@ -257,6 +259,30 @@ def qft_ops(n: int):
     for l in range(n // 2):
         ops.append(swap(l, n - l - 1))
     return ops
+
+
+def zz_ring_observable(n: int):
+    """sum_q Z_q Z_{q+1 mod n} as (masks, weights); qubit q is index bit n-1-q."""
+    masks = [(1 << (n - 1 - q)) | (1 << (n - 1 - (q + 1) % n)) for q in range(n)]
+    return masks, [1.0] * n
+
+
+def layered_cphase_ops(n: int, thetas):
+    """len(thetas) // n layers of (H on every qubit, then cphase(q, q+1 mod n,
+    theta[l, q]) for q = 0..n-1), then a final H layer.  The i-th CPHASE op
+    carries thetas[i]."""
+    thetas = np.asarray(thetas, dtype=np.float64).reshape(-1, n)
+    ops = []
+    for layer in thetas:
+        ops += [h(q) for q in range(n)]
+        ops += [cphase(q, (q + 1) % n, float(layer[q])) for q in range(n)]
+    ops += [h(q) for q in range(n)]
+    return ops
+
+
+def random_angles(count: int, seed: int) -> np.ndarray:
+    """std::uniform_real_distribution<double>(0, 2*pi) over std::mt19937(seed)."""
+    return 2.0 * np.arccos(-1.0) * mt19937_unit(seed, count)
 
 
 def random_phase(n: int, seed: int, out: np.ndarray | None = None) -> np.ndarray:
@@ -445,6 +471,22 @@ class GpuState:
         _check(lib().tmfqs_gpu_grover_run(self._h, ctypes.byref(view), a.ctypes.data_as(_U64P), len(a), iterations,
                                           1 if materialized else 0))
         return view
+
+    def adjoint_gradient(self, ops, obs_masks, obs_weights, checkpoint_every: int = 0):
+        """Runs `ops` on the current state and returns (E, dE/dtheta) for the
+        diagonal observable sum_j w_j Z(m_j): one derivative per CPHASE op, in
+        op order.  The handle holds the final state afterwards."""
+        arr = op_array(ops)
+        m = np.ascontiguousarray(np.array(obs_masks, dtype=np.uint64))
+        w = np.ascontiguousarray(np.array(obs_weights, dtype=np.float64))
+        if len(m) != len(w):
+            raise ValueError("observable masks and weights differ in length")
+        nparams = sum(1 for o in ops if o.kind == OP_CPHASE)
+        grads = np.zeros(max(1, nparams), dtype=np.float64)
+        e = ctypes.c_double()
+        _check(lib().tmfqs_gpu_adjoint_gradient(self._h, arr, len(ops), m.ctypes.data_as(_U64P), _dptr(w), len(m),
+                                                checkpoint_every, ctypes.byref(e), _dptr(grads)))
+        return e.value, grads[:nparams]
 
     def sync(self):
         _check(lib().tmfqs_gpu_sync(self._h))

@@ -1,0 +1,251 @@
+// Kernels of the adjoint (reverse-mode) gradient of a diagonal observable
+// with respect to controlled-phase angles (tmfqs_gpu_adjoint_gradient).
+//
+// k_obs_apply: lambda = O psi for a diagonal observable
+//   O = sum_j w_j Z^{m_j}  (Z^{m} = product of Z over the qubits of bit mask m:
+//   eigenvalue (-1)^popcount(x & m) on basis state x), with the expectation
+//   <psi|O|psi> accumulated in FP64.
+// k_grad_run: for a run of consecutive diagonal gates (controlled phases and
+//   phase flips), all their angle derivatives in one read of lambda and psi,
+//   then the run's inverse applied to lambda (and psi when asked).  Within a
+//   run the gates commute and have unit-modulus phases, so for every gate the
+//   derivative 2 Re <lambda_k| dU_k/dtheta |psi_{k-1}> equals
+//       2 * sum_{x: both bits set} (Im(lambda_x) Re(psi_x) - Re(lambda_x) Im(psi_x))
+//   with lambda and psi taken at the end of the run (the phases of the later
+//   gates of the run cancel in conj(lambda_x) psi_x).
+// Per-block FP64 partial sums go to a buffer the host adds in block order, so
+// the results do not depend on scheduling.
+#include <algorithm>
+#include <cmath>
+
+#include "device_common.cuh"
+#include "internal.h"
+
+namespace tqb {
+
+namespace {
+
+constexpr unsigned kAdjThreads = 256;
+constexpr unsigned kBatch = 4;      // amplitudes per thread per loop trip (observable)
+constexpr unsigned kGradBatch = 4;  // the same for the gradient runs
+
+struct ObsParams {
+	uint64_t mask[kMaxObsTerms];
+	double weight[kMaxObsTerms];
+	unsigned nterms;
+};
+
+struct RunParams {
+	uint64_t mask[kMaxDiagRun];  // controlled phase: both bit masks; flip: the basis state
+	double cr[kMaxDiagRun], ci[kMaxDiagRun];
+	int kind[kMaxDiagRun];       // DiagEntry kind
+	unsigned count;
+};
+
+__device__ __forceinline__ double block_sum(double v, double *red) {
+#pragma unroll
+	for(int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+	const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+	__syncthreads();
+	if(lane == 0) red[warp] = v;
+	__syncthreads();
+	double s = 0.0;
+	if(threadIdx.x == 0)
+		for(unsigned w = 0; w < blockDim.x / 32; ++w) s += red[w];
+	return s;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kAdjThreads) k_obs_apply(const typename Vec2<R>::type *psi, typename Vec2<R>::type *lam,
+                                                          uint64_t N, ObsParams p, double *partials) {
+	typedef typename Vec2<R>::type V;
+	__shared__ double red[kAdjThreads / 32];
+	double acc = 0.0;
+	// kBatch consecutive amplitudes per thread, loads issued together.
+	for(uint64_t x0 = gtid() * kBatch; x0 < N; x0 += gstride() * kBatch) {
+		V v[kBatch];
+#pragma unroll
+		for(unsigned u = 0; u < kBatch; ++u)
+			if(x0 + u < N) v[u] = psi[x0 + u];
+#pragma unroll
+		for(unsigned u = 0; u < kBatch; ++u) {
+			const uint64_t x = x0 + u;
+			if(x >= N) break;
+			double o = 0.0;
+			for(unsigned j = 0; j < p.nterms; ++j) o += (__popcll(x & p.mask[j]) & 1) ? -p.weight[j] : p.weight[j];
+			const double re = (double)v[u].x, im = (double)v[u].y;
+			acc += o * (re * re + im * im);
+			V l;
+			l.x = (R)(o * re);
+			l.y = (R)(o * im);
+			lam[x] = l;
+		}
+	}
+	const double s = block_sum(acc, red);
+	if(threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// Conjugate of a unit phase times v.
+template <typename V, typename R>
+__device__ __forceinline__ V mul_conj(V v, R c, R s) {
+	V r;
+	r.x = fma(c, v.x, s * v.y);
+	r.y = fma(c, v.y, -(s * v.x));
+	return r;
+}
+
+// Which entries of a run act on basis state x: an entry's condition (x
+// contains its mask, or x equals the flipped state) holds exactly when it
+// holds byte by byte, so the set of entries hitting x is the AND of one
+// 32-bit table word per index byte.  Each lane accumulates its terms in its own
+// shared-memory column (entry-major, no bank conflicts), touching only the
+// entries that hit.  A: FP32 columns for complex64 (a lane adds a few hundred
+// terms, far inside the form's tolerance), FP64 for complex128; block and grid
+// sums are FP64.
+template <typename R, typename A>
+__global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::type *lam, typename Vec2<R>::type *psi,
+                                                            uint64_t N, RunParams rp, unsigned nbytes, int uncompute_psi,
+                                                            double *partials) {
+	typedef typename Vec2<R>::type V;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	A *accs = reinterpret_cast<A *>(smem_raw);                                              // [warps][entries][32]
+	uint32_t *tab = reinterpret_cast<uint32_t *>(accs + (kAdjThreads / 32) * kMaxDiagRun * 32);  // [nbytes][256]
+	__shared__ double red[kAdjThreads / 32];
+	__shared__ R scr[kMaxDiagRun], sci[kMaxDiagRun];
+	const unsigned count = rp.count;
+	uint32_t flips = 0;
+	for(unsigned k = 0; k < count; ++k)
+		if(rp.kind[k] == kDiagFlip) flips |= 1u << k;
+	for(unsigned k = threadIdx.x; k < kMaxDiagRun; k += blockDim.x) {
+		scr[k] = k < count ? (R)rp.cr[k] : R(1);
+		sci[k] = k < count ? (R)rp.ci[k] : R(0);
+	}
+	for(unsigned e = threadIdx.x; e < nbytes * 256; e += blockDim.x) {
+		const unsigned j = e >> 8, v = e & 255u;
+		uint32_t bits = 0;
+		for(unsigned k = 0; k < count; ++k) {
+			const unsigned mb = (unsigned)(rp.mask[k] >> (8 * j)) & 255u;
+			const bool ok = ((flips >> k) & 1u) ? v == mb : (v & mb) == mb;
+			bits |= (ok ? 1u : 0u) << k;
+		}
+		tab[e] = bits;
+	}
+	for(unsigned e = threadIdx.x; e < (kAdjThreads / 32) * kMaxDiagRun * 32; e += blockDim.x) accs[e] = A(0);
+	__syncthreads();
+	const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+	A *col = accs + warp * kMaxDiagRun * 32 + lane;
+	const uint32_t all = count >= 32 ? ~0u : ((1u << count) - 1u);
+	for(uint64_t x0 = gtid() * kGradBatch; x0 < N; x0 += gstride() * kGradBatch) {
+		V lb[kGradBatch], pb[kGradBatch];
+#pragma unroll
+		for(unsigned u = 0; u < kGradBatch; ++u)
+			if(x0 + u < N) {
+				lb[u] = lam[x0 + u];
+				pb[u] = psi[x0 + u];
+			}
+#pragma unroll
+		for(unsigned u = 0; u < kGradBatch; ++u) {
+			const uint64_t x = x0 + u;
+			if(x >= N) break;
+			uint32_t hit = all;
+			for(unsigned j = 0; j < nbytes; ++j) hit &= tab[(j << 8) | ((unsigned)(x >> (8 * j)) & 255u)];
+			if(!hit) continue;
+			V l = lb[u], p = pb[u];
+			const A v = (A)l.y * (A)p.x - (A)l.x * (A)p.y;
+			for(uint32_t c = hit & ~flips; c; c &= c - 1u) col[(__ffs(c) - 1) * 32] += v;
+			// The run's inverse, last gate first.
+			for(uint32_t c = hit; c;) {
+				const int k = 31 - __clz(c);
+				c ^= 1u << k;
+				if((flips >> k) & 1u) {
+					l.x = -l.x;
+					l.y = -l.y;
+					p.x = -p.x;
+					p.y = -p.y;
+				} else {
+					const R cr = scr[k], ci = sci[k];
+					l = mul_conj(l, cr, ci);
+					if(uncompute_psi) p = mul_conj(p, cr, ci);
+				}
+			}
+			lam[x] = l;
+			if(uncompute_psi) psi[x] = p;
+		}
+	}
+	__syncthreads();
+	// Entry k: sum its column of every warp (fixed order), then the block.
+	for(unsigned k = 0; k < count; ++k) {
+		double t = 0.0;
+		const A *ck = accs + k * 32 + lane;
+		for(unsigned w = 0; w < kAdjThreads / 32; ++w) t += (double)ck[w * kMaxDiagRun * 32];
+		// Each warp holds the same t per lane; block_sum adds the lanes of every warp.
+		const double s = block_sum(warp == 0 ? t : 0.0, red);
+		if(threadIdx.x == 0) partials[blockIdx.x * kMaxDiagRun + k] = s;
+	}
+}
+
+size_t grad_smem(size_t acc_bytes, unsigned nbytes) {
+	return acc_bytes * (kAdjThreads / 32) * kMaxDiagRun * 32 + sizeof(uint32_t) * 256 * nbytes;
+}
+
+unsigned adj_blocks(const LaunchCtx &c, uint64_t N) {
+	const uint64_t per_block = (uint64_t)kAdjThreads * kGradBatch;
+	return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((N + per_block - 1) / per_block, (uint64_t)c.num_sms * 4));
+}
+
+}  // namespace
+
+unsigned adjoint_max_blocks(int num_sms) { return (unsigned)num_sms * 4; }
+
+unsigned launch_obs_apply(const LaunchCtx &c, int prec, const void *psi, void *lam, unsigned n, const uint64_t *masks,
+                          const double *weights, unsigned nterms, double *dev_partials) {
+	if(nterms == 0 || nterms > kMaxObsTerms) fail(TMFQS_ERR_INVALID_ARGUMENT, "observable: 1 to 64 terms");
+	ObsParams p{};
+	for(unsigned j = 0; j < nterms; ++j) {
+		p.mask[j] = masks[j];
+		p.weight[j] = weights[j];
+	}
+	p.nterms = nterms;
+	const uint64_t N = 1ull << n;
+	const unsigned blocks = adj_blocks(c, N);
+	if(prec == TMFQS_FP64)
+		k_obs_apply<double><<<blocks, kAdjThreads, 0, c.stream>>>(static_cast<const double2 *>(psi), static_cast<double2 *>(lam), N, p, dev_partials);
+	else
+		k_obs_apply<float><<<blocks, kAdjThreads, 0, c.stream>>>(static_cast<const float2 *>(psi), static_cast<float2 *>(lam), N, p, dev_partials);
+	check_cuda(cudaGetLastError(), "observable");
+	if(c.launches) ++*c.launches;
+	return blocks;
+}
+
+unsigned launch_grad_run(const LaunchCtx &c, int prec, void *lam, void *psi, unsigned n, const DiagEntry *entries,
+                         unsigned count, bool uncompute_psi, double *dev_partials) {
+	if(count == 0 || count > kMaxDiagRun) fail(TMFQS_ERR_LOGIC, "adjoint: diagonal run size");
+	RunParams rp{};
+	for(unsigned k = 0; k < count; ++k) {
+		rp.mask[k] = entries[k].mask;
+		rp.cr[k] = entries[k].cr;
+		rp.ci[k] = entries[k].ci;
+		rp.kind[k] = entries[k].kind;
+	}
+	rp.count = count;
+	const uint64_t N = 1ull << n;
+	const unsigned blocks = adj_blocks(c, N);
+	const int up = uncompute_psi ? 1 : 0;
+	const unsigned nbytes = (n + 7) / 8;
+	if(prec == TMFQS_FP64) {
+		const size_t smem = grad_smem(sizeof(double), nbytes);
+		check_cuda(cudaFuncSetAttribute(k_grad_run<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "gradient smem");
+		k_grad_run<double, double><<<blocks, kAdjThreads, smem, c.stream>>>(static_cast<double2 *>(lam), static_cast<double2 *>(psi), N, rp,
+		                                                                    nbytes, up, dev_partials);
+	} else {
+		const size_t smem = grad_smem(sizeof(float), nbytes);
+		check_cuda(cudaFuncSetAttribute(k_grad_run<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "gradient smem");
+		k_grad_run<float, float><<<blocks, kAdjThreads, smem, c.stream>>>(static_cast<float2 *>(lam), static_cast<float2 *>(psi), N, rp,
+		                                                                  nbytes, up, dev_partials);
+	}
+	check_cuda(cudaGetLastError(), "gradient run");
+	if(c.launches) ++*c.launches;
+	return blocks;
+}
+
+}  // namespace tqb

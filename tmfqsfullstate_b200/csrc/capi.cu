@@ -737,6 +737,237 @@ void register_inversion(tmfqs_gpu_state *h, tmfqs_register_view *v, bool materia
 
 // ===========================================================================
 // Public entry points
+// tmfqs_gpu_apply_ops: the Simulator's gate runs through the fusion planner.
+void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count) {
+	ensure_initialized(h, "operation batch");
+	if(count && !ops) fail(TMFQS_ERR_INVALID_ARGUMENT, "null op list");
+	DeviceScope d(h);
+	before_mutation(h);
+	if(!h->opt_fusion) {
+		for(size_t i = 0; i < count; ++i) {
+			validate_op(h, ops[i]);
+			Planner p(h);
+			if(ops[i].kind == TMFQS_OP_GATE) run_gate(h, ops[i].matrix, ops[i].qubits, ops[i].k);
+			else p.run_single(ops[i]);
+		}
+		check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
+		return;
+	}
+	Planner p(h);
+	size_t i = 0;
+	try {
+		while(i < count) {
+			const tmfqs_op &op = ops[i];
+			validate_op(h, op);
+			if(op.kind == TMFQS_OP_SWAP) {
+				const size_t run = swap_run(ops, i, count);
+				if(run >= 2) {
+					for(size_t j = i; j < i + run; ++j) validate_op(h, ops[j]);
+					p.flush();
+					std::vector<std::pair<unsigned, unsigned>> pairs;
+					for(size_t j = i; j < i + run; ++j) pairs.push_back({bit_of(h, ops[j].q0), bit_of(h, ops[j].q1)});
+					{
+						PassTimer timer(h, TMFQS_KT_PERMUTE, sweep_bytes(h));
+						tqb::launch_bit_permutation(ctx(h), h->precision, h->amps, h->n, pairs);
+					}
+					++h->stats.fused_passes;
+					i += run;
+					continue;
+				}
+			}
+			if(op.kind == TMFQS_OP_GATE) {
+				p.flush();
+				run_gate(h, op.matrix, op.qubits, op.k);
+				++i;
+				continue;
+			}
+			p.add(op);
+			++i;
+		}
+		p.flush();
+	} catch(const tqb::Error &) {
+		// Ops before the failing one are applied, as in the reference's
+		// sequential loop (simulator.cpp:72-82).
+		p.flush();
+		throw;
+	}
+	check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
+}
+
+// ---- adjoint gradient (tmfqs_gpu_adjoint_gradient) ----
+// A work handle of `h` (kept in *w between calls) with h's options and a state
+// of h->n qubits.
+tmfqs_gpu_state *work_handle(tmfqs_gpu_state *h, tmfqs_gpu_state *&w) {
+	if(!w) {
+		const int rc = tmfqs_gpu_create(h->precision, h->device, &w);
+		if(rc) throw tqb::Error{rc, g_last_error};
+	}
+	w->opt_fusion = h->opt_fusion;
+	w->opt_fused_qubits = h->opt_fused_qubits;
+	w->opt_exact = h->opt_exact;
+	w->opt_radix = h->opt_radix;
+	ensure_state(w, h->n);
+	w->initialized = true;
+	return w;
+}
+
+// Releases the adjoint work buffers of a handle.
+void free_adjoint_buffers(tmfqs_gpu_state *h) {
+	if(h->adj_ckpt) cudaFree(h->adj_ckpt);
+	if(h->adj_part) cudaFree(h->adj_part);
+	h->adj_ckpt = h->adj_part = nullptr;
+	h->adj_ckpt_bytes = 0;
+	if(h->adj_lam) tmfqs_gpu_destroy(h->adj_lam);
+	if(h->adj_psi) tmfqs_gpu_destroy(h->adj_psi);
+	h->adj_lam = h->adj_psi = nullptr;
+}
+
+bool is_diagonal_op(const tmfqs_op &op) { return op.kind == TMFQS_OP_CPHASE || op.kind == TMFQS_OP_PHASE_FLIP; }
+
+// Sum of per-block partials (block order), column k of a [blocks][stride] array.
+std::vector<double> read_partials(tmfqs_gpu_state *h, const double *dev, unsigned blocks, unsigned stride) {
+	std::vector<double> host((size_t)blocks * stride);
+	check_cuda(cudaMemcpyAsync(host.data(), dev, host.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+	           "partials read");
+	check_cuda(cudaStreamSynchronize(h->stream), "partials sync");
+	std::vector<double> sum(stride, 0.0);
+	for(unsigned b = 0; b < blocks; ++b)
+		for(unsigned k = 0; k < stride; ++k) sum[k] += host[(size_t)b * stride + k];
+	return sum;
+}
+
+void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, const uint64_t *masks,
+                      const double *weights, unsigned terms, size_t every, double *expectation, double *grads) {
+	ensure_initialized(h, "adjoint gradient");
+	if(count && !ops) fail(TMFQS_ERR_INVALID_ARGUMENT, "null op list");
+	if(!expectation) fail(TMFQS_ERR_INVALID_ARGUMENT, "null expectation output");
+	if(terms == 0 || terms > tqb::kMaxObsTerms) fail(TMFQS_ERR_INVALID_ARGUMENT, "observable: 1 to 64 terms");
+	if(!masks || !weights) fail(TMFQS_ERR_INVALID_ARGUMENT, "null observable");
+	for(unsigned j = 0; j < terms; ++j)
+		if(h->n < 64 && (masks[j] >> h->n) != 0) fail(TMFQS_ERR_OUT_OF_RANGE, "observable mask beyond the register");
+	std::vector<size_t> param_of(count, 0);
+	size_t nparams = 0;
+	for(size_t i = 0; i < count; ++i) {
+		if(ops[i].kind == TMFQS_OP_INVERSION) fail(TMFQS_ERR_INVALID_ARGUMENT, "adjoint gradient: inversion about the mean is not supported");
+		validate_op(h, ops[i]);
+		if(ops[i].kind == TMFQS_OP_CPHASE) param_of[i] = nparams++;
+	}
+	if(nparams && !grads) fail(TMFQS_ERR_INVALID_ARGUMENT, "null gradient output");
+	DeviceScope d(h);
+	before_mutation(h);
+	const size_t bytes = h->bytes;
+	size_t K = every;
+	if(K == 0) {
+		size_t freeb = 0, totalb = 0;
+		check_cuda(cudaMemGetInfo(&freeb, &totalb), "free memory");
+		const size_t cap = std::max<size_t>(1, (freeb / 2) / bytes);
+		K = std::max<size_t>(1, (count + cap - 1) / cap);
+	}
+	const size_t nseg = count ? (count + K - 1) / K : 0;
+	if(h->adj_ckpt_bytes < nseg * bytes) {
+		check_cuda(cudaStreamSynchronize(h->stream), "checkpoint sync");
+		if(h->adj_ckpt) cudaFree(h->adj_ckpt);
+		h->adj_ckpt = nullptr;
+		h->adj_ckpt_bytes = 0;
+		if(cudaMalloc(&h->adj_ckpt, nseg * bytes) != cudaSuccess) {
+			cudaGetLastError();
+			h->adj_ckpt = nullptr;
+			fail(TMFQS_ERR_NOMEM, "adjoint gradient: checkpoint allocation failed (raise checkpoint_every)");
+		}
+		h->adj_ckpt_bytes = nseg * bytes;
+	}
+	if(!h->adj_part &&
+	   cudaMalloc(&h->adj_part, (size_t)tqb::adjoint_max_blocks(h->num_sms) * tqb::kMaxDiagRun * sizeof(double)) != cudaSuccess) {
+		cudaGetLastError();
+		h->adj_part = nullptr;
+		fail(TMFQS_ERR_NOMEM, "adjoint gradient: scratch allocation failed");
+	}
+	unsigned char *ckb = static_cast<unsigned char *>(h->adj_ckpt);
+	double *partials = static_cast<double *>(h->adj_part);
+
+	// Forward pass, with psi saved after every segment of K ops.
+	for(size_t sidx = 0; sidx < nseg; ++sidx) {
+		const size_t a0 = sidx * K, len = std::min(K, count - a0);
+		apply_ops_body(h, ops + a0, len);
+		check_cuda(cudaMemcpyAsync(ckb + sidx * bytes, h->amps, bytes, cudaMemcpyDeviceToDevice, h->stream), "checkpoint");
+	}
+	check_cuda(cudaStreamSynchronize(h->stream), "forward sync");
+
+	struct {
+		tmfqs_gpu_state *h;
+	} lam{work_handle(h, h->adj_lam)}, psi{work_handle(h, h->adj_psi)};
+	unsigned blocks;
+	{
+		PassTimer timer(h, TMFQS_KT_ADJOINT, sweep_bytes(h));
+		blocks = tqb::launch_obs_apply(ctx(h), h->precision, h->amps, lam.h->amps, h->n, masks, weights, terms, partials);
+	}
+	*expectation = read_partials(h, partials, blocks, 1)[0];
+
+	// Backward pass: segment by segment, psi restored from its checkpoint.
+	for(size_t sidx = nseg; sidx-- > 0;) {
+		const size_t a0 = sidx * K, b0 = std::min(count, a0 + K);
+		// cp_before[i - a0]: a controlled phase lies in [a0, i).
+		std::vector<char> cp_before(b0 - a0 + 1, 0);
+		for(size_t i = a0; i < b0; ++i) cp_before[i - a0 + 1] = cp_before[i - a0] || ops[i].kind == TMFQS_OP_CPHASE;
+		check_cuda(cudaMemcpyAsync(psi.h->amps, ckb + sidx * bytes, bytes, cudaMemcpyDeviceToDevice, h->stream), "restore");
+		// psi's own passes run on its stream.
+		check_cuda(cudaStreamSynchronize(h->stream), "restore sync");
+		size_t i = b0;
+		while(i > a0) {
+			const bool diag = is_diagonal_op(ops[i - 1]);
+			size_t j = i;
+			while(j > a0 && is_diagonal_op(ops[j - 1]) == diag) --j;  // the run [j, i)
+			if(diag) {
+				for(size_t e = i; e > j;) {
+					const size_t st = std::max(j, e > tqb::kMaxDiagRun ? e - tqb::kMaxDiagRun : 0);
+					std::vector<tqb::DiagEntry> ent;
+					for(size_t k = st; k < e; ++k) {
+						const tmfqs_op &op = ops[k];
+						if(op.kind == TMFQS_OP_CPHASE)
+							ent.push_back({tqb::kDiagCPhase, (1ull << bit_of(h, op.q0)) | (1ull << bit_of(h, op.q1)),
+							               std::cos(op.theta), std::sin(op.theta)});
+						else
+							ent.push_back({tqb::kDiagFlip, op.state, 1.0, 0.0});
+					}
+					const bool need_psi = cp_before[st - a0] != 0;
+					{
+						PassTimer timer(h, TMFQS_KT_ADJOINT, sweep_bytes(h) * (need_psi ? 2.0 : 1.5));
+						blocks = tqb::launch_grad_run(ctx(h), h->precision, lam.h->amps, psi.h->amps, h->n, ent.data(),
+						                              (unsigned)ent.size(), need_psi, partials);
+					}
+					const std::vector<double> g = read_partials(h, partials, blocks, tqb::kMaxDiagRun);
+					for(size_t k = st; k < e; ++k)
+						if(ops[k].kind == TMFQS_OP_CPHASE) grads[param_of[k]] = 2.0 * g[k - st];
+					e = st;
+				}
+			} else {
+				// Inverse of the run, last op first.
+				std::vector<tmfqs_op> inv;
+				std::vector<std::vector<double>> mats;
+				for(size_t k = i; k-- > j;) {
+					tmfqs_op op = ops[k];
+					if(op.kind == TMFQS_OP_GATE) {
+						const size_t dim = size_t(1) << op.k;
+						std::vector<double> m(2 * dim * dim);
+						for(size_t r = 0; r < dim; ++r)
+							for(size_t c = 0; c < dim; ++c) {
+								m[2 * (r * dim + c)] = op.matrix[2 * (c * dim + r)];
+								m[2 * (r * dim + c) + 1] = -op.matrix[2 * (c * dim + r) + 1];
+							}
+						mats.push_back(std::move(m));
+						op.matrix = mats.back().data();
+					}
+					inv.push_back(op);
+				}
+				apply_ops_body(lam.h, inv.data(), inv.size());
+				if(cp_before[j - a0]) apply_ops_body(psi.h, inv.data(), inv.size());
+			}
+			i = j;
+		}
+	}
+	check_cuda(cudaStreamSynchronize(h->stream), "backward sync");
+}
+
 // ===========================================================================
 extern "C" {
 
@@ -785,6 +1016,7 @@ int tmfqs_gpu_destroy(tmfqs_gpu_state *h) {
 			cudaEventDestroy(t.stop);
 		}
 		tqb::seq_scratch_free(h->seq);
+		free_adjoint_buffers(h);
 		if(h->amps) cudaFree(h->amps);
 		if(h->dev_small) cudaFree(h->dev_small);
 		if(h->dev_prog) cudaFree(h->dev_prog);
@@ -1160,61 +1392,7 @@ int tmfqs_gpu_gate(tmfqs_gpu_state *h, const double *matrix, const unsigned *qub
 }
 
 int tmfqs_gpu_apply_ops(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count) {
-	return guarded([&] {
-		ensure_initialized(h, "operation batch");
-		if(count && !ops) fail(TMFQS_ERR_INVALID_ARGUMENT, "null op list");
-		DeviceScope d(h);
-		before_mutation(h);
-		if(!h->opt_fusion) {
-			for(size_t i = 0; i < count; ++i) {
-				validate_op(h, ops[i]);
-				Planner p(h);
-				if(ops[i].kind == TMFQS_OP_GATE) run_gate(h, ops[i].matrix, ops[i].qubits, ops[i].k);
-				else p.run_single(ops[i]);
-			}
-			check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
-			return;
-		}
-		Planner p(h);
-		size_t i = 0;
-		try {
-			while(i < count) {
-				const tmfqs_op &op = ops[i];
-				validate_op(h, op);
-				if(op.kind == TMFQS_OP_SWAP) {
-					const size_t run = swap_run(ops, i, count);
-					if(run >= 2) {
-						for(size_t j = i; j < i + run; ++j) validate_op(h, ops[j]);
-						p.flush();
-						std::vector<std::pair<unsigned, unsigned>> pairs;
-						for(size_t j = i; j < i + run; ++j) pairs.push_back({bit_of(h, ops[j].q0), bit_of(h, ops[j].q1)});
-						{
-							PassTimer timer(h, TMFQS_KT_PERMUTE, sweep_bytes(h));
-							tqb::launch_bit_permutation(ctx(h), h->precision, h->amps, h->n, pairs);
-						}
-						++h->stats.fused_passes;
-						i += run;
-						continue;
-					}
-				}
-				if(op.kind == TMFQS_OP_GATE) {
-					p.flush();
-					run_gate(h, op.matrix, op.qubits, op.k);
-					++i;
-					continue;
-				}
-				p.add(op);
-				++i;
-			}
-			p.flush();
-		} catch(const tqb::Error &) {
-			// Ops before the failing one are applied, as in the reference's
-			// sequential loop (simulator.cpp:72-82).
-			p.flush();
-			throw;
-		}
-		check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
-	});
+	return guarded([&] { apply_ops_body(h, ops, count); });
 }
 
 int tmfqs_gpu_grover_run(tmfqs_gpu_state *h, tmfqs_register_view *view, const uint64_t *marked, size_t count,
@@ -1252,6 +1430,15 @@ int tmfqs_sample_static(const void *device_amps, int precision, unsigned num_qub
 			tqb::seq_sample_static(precision, device_amps, num_qubits, rnd, static_cast<cudaStream_t>(stream));
 		if(r.index >= (1ull << num_qubits)) fail(TMFQS_ERR_RUNTIME, "tmfqs_sample_static: cumulative probability did not reach sample");
 		*index_out = r.index;
+	});
+}
+
+int tmfqs_gpu_adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, const uint64_t *obs_masks,
+                               const double *obs_weights, unsigned obs_terms, size_t checkpoint_every,
+                               double *expectation, double *grads) {
+	return guarded([&] {
+		require_handle(h);
+		adjoint_gradient(h, ops, count, obs_masks, obs_weights, obs_terms, checkpoint_every, expectation, grads);
 	});
 }
 

@@ -84,6 +84,11 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 	__shared__ double2 twa[64], twb[32];
 	__shared__ int tla[6], tlb[5];
 	__shared__ int tna, tnb;
+	// A chunk of a run of diagonal ops, staged for the per-amplitude loop.
+	constexpr unsigned kDiagChunk = 32;
+	__shared__ uint64_t dmask[kDiagChunk];
+	__shared__ double2 dph[kDiagChunk];
+	__shared__ int dflip[kDiagChunk];
 	for(unsigned h = threadIdx.x; h < nhi; h += blockDim.x) {
 		uint64_t v = 0;
 		for(unsigned i = 0; i < g.K - g.m; ++i)
@@ -287,29 +292,44 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 					__syncthreads();
 					break;
 				}
-				case kFCP: {
-					const R pr = (R)op.cr, pi = (R)op.ci;
-					for(unsigned j = threadIdx.x; j < T; j += blockDim.x) {
-						if(((base | scatter(j)) & op.mask) != op.mask) continue;
-						V v = s[j];
-						if(v.x == R(0) && v.y == R(0)) continue;
-						cmul_ref(pr, pi, v.x, v.y);
-						s[j] = v;
-					}
-					// Diagonal ops keep the thread->amplitude ownership; a barrier
-					// is needed only before the next pair operation.
-					if(k + 1 == g.nops || (ops[k + 1].kind != kFCP && ops[k + 1].kind != kFFlip)) __syncthreads();
-					break;
-				}
+				case kFCP:
 				case kFFlip: {
-					for(unsigned j = threadIdx.x; j < T; j += blockDim.x) {
-						if((base | scatter(j)) != op.state) continue;
-						V v = s[j];
-						v.x = -v.x;
-						v.y = -v.y;
-						s[j] = v;
+					// A run of consecutive diagonal ops in one sweep: each amplitude
+					// still receives them one by one, in circuit order.
+					unsigned e = k + 1;
+					while(e < g.nops && e - k < kDiagChunk && (ops[e].kind == kFCP || ops[e].kind == kFFlip)) ++e;
+					const unsigned cnt = e - k;
+					for(unsigned q = threadIdx.x; q < cnt; q += blockDim.x) {
+						const FusedOp d = ops[k + q];
+						dflip[q] = d.kind == kFFlip;
+						dmask[q] = d.kind == kFFlip ? d.state : d.mask;
+						dph[q] = make_double2(d.cr, d.ci);
 					}
-					if(k + 1 == g.nops || (ops[k + 1].kind != kFCP && ops[k + 1].kind != kFFlip)) __syncthreads();
+					__syncthreads();
+					for(unsigned j = threadIdx.x; j < T; j += blockDim.x) {
+						const uint64_t x = base | scatter(j);
+						V v = s[j];
+						bool dirty = false;
+						for(unsigned q = 0; q < cnt; ++q) {
+							const uint64_t m = dmask[q];
+							if(!dflip[q]) {
+								// Zero amplitudes are skipped (dense_state_backend.cpp:299).
+								if((x & m) != m || (v.x == R(0) && v.y == R(0))) continue;
+								const double2 ph = dph[q];
+								cmul_ref((R)ph.x, (R)ph.y, v.x, v.y);
+							} else {
+								if(x != m) continue;
+								v.x = -v.x;
+								v.y = -v.y;
+							}
+							dirty = true;
+						}
+						if(dirty) s[j] = v;
+					}
+					// Diagonal ops keep the thread->amplitude ownership; the barrier
+					// also frees the staged chunk.
+					__syncthreads();
+					k = e - 1;
 					break;
 				}
 				default:

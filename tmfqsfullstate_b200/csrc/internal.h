@@ -144,6 +144,31 @@ void launch_fused_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &p
 bool launch_radix_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, void *&dev_prog,
                        size_t &dev_prog_bytes);
 
+// ---------------------------------------------------------------------------
+// Adjoint gradient (adjoint.cu)
+// ---------------------------------------------------------------------------
+constexpr unsigned kMaxObsTerms = 64;  // Z-string terms of a diagonal observable
+constexpr unsigned kMaxDiagRun = 32;   // diagonal gates per gradient pass
+
+enum DiagKind : int { kDiagCPhase = 0, kDiagFlip = 1 };
+
+struct DiagEntry {
+	int kind;       // DiagKind
+	uint64_t mask;  // controlled phase: both bit masks; flip: the basis state
+	double cr, ci;  // controlled phase: cos(theta), sin(theta)
+};
+
+// Upper bound on the blocks (and so the per-block partial sums) of a launch.
+unsigned adjoint_max_blocks(int num_sms);
+// lambda = O psi; writes one FP64 partial of <psi|O|psi> per block; returns
+// the number of blocks.
+unsigned launch_obs_apply(const LaunchCtx &c, int prec, const void *psi, void *lam, unsigned n, const uint64_t *masks,
+                          const double *weights, unsigned nterms, double *dev_partials);
+// Angle-derivative sums of a diagonal run (partials[block * kMaxDiagRun + k]),
+// then the run's inverse on lambda (and on psi if asked); returns the blocks.
+unsigned launch_grad_run(const LaunchCtx &c, int prec, void *lam, void *psi, unsigned n, const DiagEntry *entries,
+                         unsigned count, bool uncompute_psi, double *dev_partials);
+
 // Involutive permutation of bit positions (disjoint transpositions), as one
 // in-place pass: amplitude x moves to perm(x).  pairs[i] = (p, q) bit positions.
 void launch_bit_permutation(const LaunchCtx &c, int prec, void *a, unsigned n,
@@ -198,6 +223,12 @@ struct tmfqs_gpu_state {
 	bool opt_grover_fusion = true;
 	bool opt_exact = true;
 	bool opt_radix = true;  // fast forms: radix passes where the program allows
+	// Adjoint-gradient work buffers, kept for the next call (freed by destroy):
+	// psi checkpoints, FP64 partial sums, and the lambda / psi work states.
+	void *adj_ckpt = nullptr;
+	size_t adj_ckpt_bytes = 0;
+	void *adj_part = nullptr;
+	tmfqs_gpu_state *adj_lam = nullptr, *adj_psi = nullptr;
 };
 
 #endif

@@ -64,6 +64,7 @@ struct RadixStage {
 	uint32_t pre_slot, pre_mask;    // first factor slot; bit 0 constant factor, bit i+1 register bit i
 	uint32_t post_slot, post_mask;
 	uint32_t direct;                // last stage: store to HBM from registers
+	uint32_t post_xfirst, post_xcount;  // per-thread terms of the post constant factor
 };
 
 // One phase term of a factor slot: theta when all its bits are set.  bit1 is
@@ -73,12 +74,17 @@ constexpr uint32_t kNoBit = 0xffffffffu;
 struct RadixTerm {
 	uint32_t bit0, bit1;
 	double theta;
+	uint32_t outer;  // thread terms: bit 0 / bit 1 set when bit0 / bit1 is an outer (global) bit
+	uint32_t pad;
+	double c, s;     // thread terms: cos(theta), sin(theta)
 };
 
 struct RadixSlot {
 	uint32_t a_first, a_count;  // terms on A-range local bits
 	uint32_t b_first, b_count;  // terms on B-range local bits
 	uint32_t o_first, o_count;  // terms on outer bits
+	uint32_t x_first, x_count;  // constant slot: two-bit terms the tables cannot hold (a local bit with an
+	                            // outer bit, or local bits of both tables), evaluated per thread
 	double scale;               // real factor folded into the slot (1, or the pass's Hadamard scale)
 };
 
@@ -283,17 +289,38 @@ __device__ __forceinline__ void qft_dispatch(V (&v)[1 << RB], unsigned d, const 
 	}
 }
 
+// The constant factor times its per-thread terms (two-bit phases the tables
+// cannot hold); kept out of line, off the common path.
+template <typename V>
+__device__ __noinline__ V thread_terms(V f, const RadixTerm *terms, unsigned first, unsigned count, unsigned jt,
+                                       uint64_t base) {
+	for(unsigned t = 0; t < count; ++t) {
+		const RadixTerm tm = terms[first + t];
+		const bool on0 = (tm.outer & 1u) ? ((base >> tm.bit0) & 1ull) : ((jt >> tm.bit0) & 1u);
+		const bool on1 = (tm.outer & 2u) ? ((base >> tm.bit1) & 1ull) : ((jt >> tm.bit1) & 1u);
+		if(on0 && on1) {
+			V w;
+			w.x = (decltype(w.x))tm.c;
+			w.y = (decltype(w.y))tm.s;
+			f = vmul(f, w);
+		}
+	}
+	return f;
+}
+
 // Multiplies v[r] by the product of the active factors of a slot group:
 // factor 0 for every r (if bit 0 of mask), factor i+1 for r with bit i.
 template <typename V, int RB>
 __device__ __forceinline__ void apply_factors(V (&v)[1 << RB], const RadixSmem<V> &sh, unsigned slot0, unsigned mask,
-                                              unsigned ia, unsigned ib, unsigned lo, unsigned nb) {
+                                              unsigned ia, unsigned ib, unsigned lo, unsigned nb, const RadixTerm *terms,
+                                              unsigned xfirst, unsigned xcount, unsigned jt, uint64_t base) {
 	V f[RB + 1];
 	unsigned s = slot0;
 #pragma unroll
 	for(int i = 0; i <= RB; ++i) {
 		if((mask >> i) & 1u) {
 			f[i] = vmul(sh.A[(s << lo) + ia], sh.Bt[s * nb + ib]);
+			if(i == 0 && xcount) f[0] = thread_terms(f[0], terms, xfirst, xcount, jt, base);
 			++s;
 		} else {
 			f[i].x = 1;
@@ -451,7 +478,7 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 #pragma unroll
 			for(int r = 0; r < (1 << RB); ++r) v[r] = tile[addr(r)];
 			const unsigned ia = jt & ((1u << g.lo) - 1u), ib = jt >> g.lo;
-			if(S.pre_mask) apply_factors<V, RB>(v, sh, S.pre_slot, S.pre_mask, ia, ib, g.lo, nb);
+			if(S.pre_mask) apply_factors<V, RB>(v, sh, S.pre_slot, S.pre_mask, ia, ib, g.lo, nb, gterms, 0, 0, jt, cbase);
 			for(unsigned k = S.first; k < S.first + S.count; ++k) {
 				const uint32_t it = sh.items[k];
 				const unsigned kind = it & 0xffu, b = (it >> 8) & 0xffu;
@@ -465,7 +492,9 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 					rbfly_dispatch<V, RB>(v, b, kind == kRIButterflyTw ? tb : nullptr);
 				}
 			}
-			if(S.post_mask) apply_factors<V, RB>(v, sh, S.post_slot, S.post_mask, ia, ib, g.lo, nb);
+			if(S.post_mask)
+				apply_factors<V, RB>(v, sh, S.post_slot, S.post_mask, ia, ib, g.lo, nb, gterms, S.post_xfirst, S.post_xcount, jt,
+				                     cbase);
 			const bool last = st + 1 == g.nstages;
 			if(last && tid < g.nslots) {
 				// Next tile's outer phases (this tile's tables are already built).
@@ -741,16 +770,18 @@ bool build_radix_program(const FusedPass &pass, unsigned K, size_t vbytes, Radix
 				const bool sc = i == 0 && with_scale;
 				if(grp[i].empty() && !sc) continue;
 				mask |= 1u << i;
-				std::vector<RadixTerm> A, B, O;
+				std::vector<RadixTerm> A, B, O, X;
 				for(const STerm &t : grp[i]) {
 					const uint32_t y = t.two ? t.y.idx : kNoBit;
-					if(t.two && t.x.local != t.y.local) return false;  // local x outer products
-					if(!t.x.local) {
-						O.push_back(RadixTerm{t.x.idx, y, t.theta});
+					const bool cross = t.two && (t.x.local != t.y.local || (t.x.local && (t.x.idx < g.lo) != (t.y.idx < g.lo)));
+					if(cross) {
+						// Only the constant slot holds two-bit terms.
+						X.push_back(RadixTerm{t.x.idx, t.y.idx, t.theta, (t.x.local ? 0u : 1u) | (t.y.local ? 0u : 2u), 0,
+						                      std::cos(t.theta), std::sin(t.theta)});
+					} else if(!t.x.local) {
+						O.push_back(RadixTerm{t.x.idx, y, t.theta, 0, 0, 0.0, 0.0});
 					} else {
-						const bool xa = t.x.idx < g.lo;
-						if(t.two && (t.y.idx < g.lo) != xa) return false;  // across the two tables
-						(xa ? A : B).push_back(RadixTerm{t.x.idx, y, t.theta});
+						(t.x.idx < g.lo ? A : B).push_back(RadixTerm{t.x.idx, y, t.theta, 0, 0, 0.0, 0.0});
 					}
 				}
 				RadixSlot sl{};
@@ -764,11 +795,18 @@ bool build_radix_program(const FusedPass &pass, unsigned K, size_t vbytes, Radix
 				sl.o_first = (uint32_t)P.terms.size();
 				sl.o_count = (uint32_t)O.size();
 				P.terms.insert(P.terms.end(), O.begin(), O.end());
+				sl.x_first = (uint32_t)P.terms.size();
+				sl.x_count = (uint32_t)X.size();
+				P.terms.insert(P.terms.end(), X.begin(), X.end());
 				P.slots.push_back(sl);
 			}
 			return true;
 		};
 		if(!emit(pre, false, S.pre_slot, S.pre_mask) || !emit(post, last, S.post_slot, S.post_mask)) return false;
+		if(S.post_mask & 1u) {
+			S.post_xfirst = P.slots[S.post_slot].x_first;
+			S.post_xcount = P.slots[S.post_slot].x_count;
+		}
 		// Direct stores from the last stage when the lowest non-register local
 		// bits (the lanes) cover 32 contiguous bytes of the state.
 		if(last) {
