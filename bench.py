@@ -26,6 +26,16 @@ between steps.
           backward/forward cost, and the error against the reference's
           parameter-shift gradients (tests/golden/adjoint_ps_n24.json) and
           FP64 central finite differences on the same 32 angles.
+  qft32   configuration 3: QFT on 32 qubits, complex64 (32 GiB) beside the
+          complex128 plain form (64 GiB) as its FP64 oracle, for the pattern
+          input (uniform over k = 0 mod 2^10; analytic answer) and a random-phase
+          input generated on the device (torch.Generator, seed 123456 -- the
+          reference's host generator would take minutes and 64 GiB of host
+          memory at this size).
+  grover30 configuration 4: Grover search on 30 qubits, 4 marked states,
+          12867 iterations, lazy and materialised diffusion, complex64 (8 GiB)
+          and complex128 (16 GiB): per-iteration time and the marked-state
+          probability error of complex64.
   --impl reference   the reference's own Dense CPU path (oracle/_ref, compiled
           from the reference sources) on this host, on a bounded prefix of the
           same circuit.
@@ -65,6 +75,7 @@ def parse_args():
     p.add_argument("--form-steps", type=int, default=3)
     p.add_argument("--no-forms", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-configs", action="store_true", help="skip the QFT-32 and Grover-30 sections")
     return p.parse_args()
 
 
@@ -275,6 +286,142 @@ def run_adjoint(tq, torch, device, reps=3):
     return out
 
 
+def _timed_ops(torch, g, ops):
+    stream = torch.cuda.ExternalStream(g.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g.sync()
+    e0.record(stream)
+    g.apply_ops(ops)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _compare(torch, a, b, chunk=1 << 27):
+    """Fidelity and relative L2 error of two interleaved device states (FP64 accumulation)."""
+    dot_re = dot_im = na = nb = diff = 0.0
+    for i in range(0, a.numel(), 2 * chunk):
+        x = a[i:i + 2 * chunk].double().view(-1, 2)
+        y = b[i:i + 2 * chunk].double().view(-1, 2)
+        dot_re += float((x[:, 0] * y[:, 0] + x[:, 1] * y[:, 1]).sum())
+        dot_im += float((x[:, 0] * y[:, 1] - x[:, 1] * y[:, 0]).sum())
+        na += float((x * x).sum())
+        nb += float((y * y).sum())
+        diff += float(((x - y) ** 2).sum())
+    return (dot_re ** 2 + dot_im ** 2) / (na * nb), (diff / na) ** 0.5
+
+
+def _pattern_error(torch, t, n, m, chunk=1 << 27):
+    """max |a_y - expected_y| for the QFT of the uniform state over k = 0 mod 2^m."""
+    peak = 2.0 ** (-m / 2.0)
+    step = 1 << (n - m)
+    worst = 0.0
+    for i in range(0, t.numel() // 2, chunk):
+        x = t[2 * i:2 * (i + chunk)].double().view(-1, 2)
+        idx = torch.arange(i, i + x.shape[0], device=x.device)
+        exp_re = torch.where(idx % step == 0, torch.full_like(x[:, 0], peak), torch.zeros_like(x[:, 0]))
+        worst = max(worst, float(torch.maximum((x[:, 0] - exp_re).abs(), x[:, 1].abs()).max()))
+    return worst
+
+
+def run_qft32(tq, torch, device, peak):
+    import numpy as np
+
+    n, m = 32, 10
+    ops = tq.qft_ops(n)
+    upd = len(ops) * (1 << n)
+    out = {"n_qubits": n, "circuit_ops": len(ops)}
+    g64 = tq.GpuState(tq.FP32, device)
+    g128 = tq.GpuState(tq.FP64, device)
+    try:
+        for inp in ("pattern", "random_phase"):
+            if inp == "pattern":
+                states = np.arange(0, 1 << n, 1 << m, dtype=np.uint64)
+                g64.init_uniform(n, states)
+                g128.init_uniform(n, states)
+            else:
+                g64.init_zero(n)
+                g128.init_zero(n)
+                t64, t128 = g64.tensor(), g128.tensor()
+                gen = torch.Generator(device=t128.device)
+                gen.manual_seed(SEED)
+                two_pi, norm = 2.0 * np.arccos(-1.0), 2.0 ** (-n / 2.0)
+                chunk = 1 << 26
+                for i in range(0, 1 << n, chunk):
+                    th = torch.rand(chunk, dtype=torch.float64, device=t128.device, generator=gen) * two_pi
+                    blk = torch.stack([torch.cos(th), torch.sin(th)], dim=1).reshape(-1) * norm
+                    t128[2 * i:2 * (i + chunk)].copy_(blk)
+                    t64[2 * i:2 * (i + chunk)].copy_(blk.float())
+                del t64, t128
+                torch.cuda.synchronize()
+            res = {}
+            for name, g, sweep in (("complex64_radix", g64, 16 << n), ("complex128_plain", g128, 32 << n)):
+                g.reset_stats()
+                g.set_option(tq.OPT_KERNEL_TIMING, 1)
+                ms = _timed_ops(torch, g, ops)
+                kt = g.kernel_times()
+                g.set_option(tq.OPT_KERNEL_TIMING, 0)
+                passes = kt["fused"]["launches"] + kt["permute"]["launches"]
+                res[name] = {"ms_per_qft": ms, "value": upd / (ms / 1e3), "sweeps": passes,
+                             "hbm_frac_whole_qft": passes * sweep / (ms / 1e3) / 1e9 / peak}
+            fid, rel = _compare(torch, g128.tensor(), g64.tensor())
+            res["fidelity_c64_vs_c128"] = fid
+            res["rel_l2_c64_vs_c128"] = rel
+            res["speedup_c64_vs_c128_plain"] = res["complex128_plain"]["ms_per_qft"] / res["complex64_radix"]["ms_per_qft"]
+            if inp == "pattern":
+                res["max_abs_err_vs_analytic"] = {"complex64": _pattern_error(torch, g64.tensor(), n, m),
+                                                  "complex128": _pattern_error(torch, g128.tensor(), n, m)}
+            out[inp] = res
+            torch.cuda.empty_cache()
+    finally:
+        g64.close()
+        g128.close()
+    return out
+
+
+def run_grover30(tq, device, peak):
+    import math
+
+    n, nm = 30, 4
+    marked = [int(v) for v in tq.uniform_states(SEED, nm, 0, (1 << n) - 1)]
+    iters = int(math.floor(math.pi / 4.0 * math.sqrt((1 << n) / nm)))
+    out = {"n_qubits": n, "marked": marked, "iterations": iters}
+    probs = {}
+    for name, prec, b in (("complex64", tq.FP32, 8), ("complex128", tq.FP64, 16)):
+        g = tq.GpuState(prec, device)
+        try:
+            for mat in (False, True):
+                g.init_basis(n, 0)
+                g.apply_ops([tq.h(q) for q in range(n)])
+                view = tq.RegisterView.fresh()
+                g.sync()
+                t0 = time.perf_counter()
+                g.grover_run(view, marked, iters, mat)
+                g.sync()
+                secs = time.perf_counter() - t0
+                p = 0.0
+                for s in marked:
+                    re, im = g.amplitude(s)
+                    if view.overlay:
+                        re, im = ((view.scale_re * re - view.scale_im * im) + view.bias_re,
+                                  (view.scale_re * im + view.scale_im * re) + view.bias_im)
+                    p += re * re + im * im
+                form = "materialized" if mat else "lazy"
+                sweep = 2 * b * (1 << n)
+                d = {"seconds": secs, "us_per_iteration": secs / iters * 1e6, "p_marked": p}
+                if mat:
+                    # All iterations in one temporal pass: one sweep instead of one per iteration.
+                    d["sweep_equivalent_frac"] = iters * sweep / secs / 1e9 / peak
+                    d["hbm_frac_actual"] = sweep / secs / 1e9 / peak
+                out[f"{name}_{form}"] = d
+                probs[(name, form)] = p
+        finally:
+            g.close()
+    for form in ("lazy", "materialized"):
+        out[f"p_marked_err_c64_{form}"] = abs(probs[("complex64", form)] - probs[("complex128", form)])
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -378,6 +525,9 @@ def run_ours(args):
     adjoint = None
     if rank == 0 and not args.no_adjoint:
         adjoint = run_adjoint(tq, torch, local)
+    configs = None
+    if rank == 0 and not args.no_configs:
+        configs = {"qft32": run_qft32(tq, torch, local, peak), "grover30": run_grover30(tq, local, peak)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -394,7 +544,7 @@ def run_ours(args):
                     "ms_per_step": e2e_s * 1e3},
             "gpu_launches": int(stats["kernel_launches"]),
             "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "forms": forms,
-            "adjoint": adjoint,
+            "adjoint": adjoint, "configs": configs,
             "kernel_times_ms": {k: round(v["ms"], 3) for k, v in kt.items() if v["launches"]},
             "check": {"total_probability": total, "measured": measured,
                       "reference_golden": {"total_probability": 0.99999999999986022, "measured": 138222191}},

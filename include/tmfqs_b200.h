@@ -263,6 +263,11 @@ TMFQS_API int tmfqs_random_phase(unsigned num_qubits, uint32_t seed, double *hos
 /* The first `count` draws of Mt19937RandomSource(seed).nextUnitDouble(),
  * core/random.h:32-58 -- the draws measure() consumes. */
 TMFQS_API int tmfqs_mt19937_unit(uint32_t seed, uint64_t count, double *host_out);
+/* `count` distinct basis states drawn by std::uniform_int_distribution<uint64_t>(lo, hi)
+ * over std::mt19937_64(seed), in draw order (repeats skipped): the marked
+ * states of the 30-qubit, 4-marked-state Grover benchmark.  No reference
+ * counterpart (its CLIs take the marked states as arguments). */
+TMFQS_API int tmfqs_uniform_states(uint64_t seed, uint64_t count, uint64_t lo, uint64_t hi, uint64_t *host_out);
 
 /* ---- instrumentation -------------------------------------------------- */
 TMFQS_API int tmfqs_gpu_stats(tmfqs_gpu_state *h, tmfqs_stats *out);

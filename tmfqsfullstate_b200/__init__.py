@@ -170,6 +170,7 @@ SIGNATURES = {
     "tmfqs_random_phase": [_UI, ctypes.c_uint32, _DP],
     "tmfqs_sample_static": [ctypes.c_void_p, ctypes.c_int, _UI, _D, ctypes.c_void_p, _U64P],
     "tmfqs_mt19937_unit": [ctypes.c_uint32, _U64, _DP],
+    "tmfqs_uniform_states": [_U64, _U64, _U64, _U64, _U64P],
 }
 
 _lib = None
@@ -280,6 +281,13 @@ def layered_cphase_ops(n: int, thetas):
     return ops
 
 
+def uniform_states(seed: int, count: int, lo: int, hi: int) -> np.ndarray:
+    """`count` distinct draws of std::uniform_int_distribution<uint64_t>(lo, hi) over std::mt19937_64(seed)."""
+    out = np.zeros(max(1, count), dtype=np.uint64)
+    _check(lib().tmfqs_uniform_states(seed, count, lo, hi, out.ctypes.data_as(_U64P)))
+    return out[:count]
+
+
 def random_angles(count: int, seed: int) -> np.ndarray:
     """std::uniform_real_distribution<double>(0, 2*pi) over std::mt19937(seed)."""
     return 2.0 * np.arccos(-1.0) * mt19937_unit(seed, count)
@@ -325,6 +333,7 @@ class GpuState:
     """One register's state vector in HBM (a tmfqs_gpu_state handle)."""
 
     def __init__(self, precision: int = FP64, device: int = 0, _handle=None):
+        self.device = device
         self._h = ctypes.c_void_p()
         if _handle is not None:
             self._h = _handle
@@ -352,7 +361,12 @@ class GpuState:
     def clone(self) -> "GpuState":
         out = ctypes.c_void_p()
         _check(lib().tmfqs_gpu_clone(self._h, ctypes.byref(out)))
-        return GpuState(_handle=out)
+        return GpuState(device=self.device, _handle=out)
+
+    def precision(self) -> int:
+        v = ctypes.c_int()
+        _check(lib().tmfqs_gpu_precision(self._h, ctypes.byref(v)))
+        return v.value
 
     @property
     def num_qubits(self) -> int:
@@ -487,6 +501,23 @@ class GpuState:
         _check(lib().tmfqs_gpu_adjoint_gradient(self._h, arr, len(ops), m.ctypes.data_as(_U64P), _dptr(w), len(m),
                                                 checkpoint_every, ctypes.byref(e), _dptr(grads)))
         return e.value, grads[:nparams]
+
+    def tensor(self):
+        """A torch tensor viewing the handle's device state (interleaved re, im;
+        float64 for FP64 handles, float32 for FP32) without a copy.  It is valid
+        until the state is re-allocated or the handle closed; queued work on the
+        handle's stream must be synchronised before torch reads it."""
+        import torch
+
+        self.sync()
+        ptr, nbytes = self.device_buffer()
+        dt = "<f8" if self.precision() == FP64 else "<f4"
+        elem = 8 if dt == "<f8" else 4
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (nbytes // elem,), "typestr": dt, "data": (ptr, False), "version": 2}
+
+        return torch.as_tensor(_View(), device=torch.device("cuda", self.device))
 
     def sync(self):
         _check(lib().tmfqs_gpu_sync(self._h))

@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <random>
 #include <string>
+#include <unordered_set>
 
 #include "../../include/tmfqs_b200.h"
 
@@ -35,6 +36,18 @@ TMFQS_API int tmfqs_mt19937_unit(uint32_t seed, uint64_t count, double *host_out
 	std::mt19937 gen(seed);
 	std::uniform_real_distribution<double> unit(0.0, 1.0);
 	for(uint64_t i = 0; i < count; ++i) host_out[i] = unit(gen);
+	return TMFQS_OK;
+}
+
+TMFQS_API int tmfqs_uniform_states(uint64_t seed, uint64_t count, uint64_t lo, uint64_t hi, uint64_t *host_out) {
+	if((!host_out && count) || lo > hi || (hi - lo < UINT64_MAX && count > hi - lo + 1)) return TMFQS_ERR_INVALID_ARGUMENT;
+	std::mt19937_64 gen(seed);
+	std::uniform_int_distribution<uint64_t> dist(lo, hi);
+	std::unordered_set<uint64_t> seen;
+	for(uint64_t i = 0; i < count;) {
+		const uint64_t v = dist(gen);
+		if(seen.insert(v).second) host_out[i++] = v;
+	}
 	return TMFQS_OK;
 }
 
