@@ -63,7 +63,8 @@ def test_grover30_reference_prefix(form):
         assert meas == ref["measured"]
 
 
-def test_grover30_c64_tracks_c128():
+@pytest.mark.parametrize("materialized", [False, True])
+def test_grover30_c64_tracks_c128(materialized):
     marked = marked30()
     iters = int(math.floor(math.pi / 4.0 * math.sqrt((1 << N30) / len(marked))))
     assert iters == 12867
@@ -73,10 +74,15 @@ def test_grover30_c64_tracks_c128():
             g.init_basis(N30, 0)
             g.apply_ops([tq.h(q) for q in range(N30)])
             view = tq.RegisterView.fresh()
-            g.grover_run(view, marked, iters, False)
+            g.grover_run(view, marked, iters, materialized)
             p[prec] = sum(a * a + b * b for a, b in (logical(g, view, s) for s in marked))
+            if materialized:
+                # An unmarked amplitude as well.
+                p[(prec, "u")] = logical(g, view, 12345)
     assert p[tq.FP64] > 0.999
     assert abs(p[tq.FP32] - p[tq.FP64]) < 1e-5
+    if materialized:
+        assert abs(p[(tq.FP32, "u")][0] - p[(tq.FP64, "u")][0]) < 1e-9
 
 
 def test_qft30_pattern_known_answer_c64():

@@ -114,3 +114,24 @@ def test_c64_grover(materialized):
                 re, im = (v.scale_re * re - v.scale_im * im) + v.bias_re, (v.scale_re * im + v.scale_im * re) + v.bias_im
             pr = r.amplitude(s)
             assert abs(re * re + im * im - (pr[0] ** 2 + pr[1] ** 2)) < 1e-5
+
+
+@pytest.mark.parametrize("materialized", [True, False])
+def test_fast_fp64_grover(materialized):
+    """The fast FP64 form's Grover run (closed-form materialised pass) against the oracle."""
+    n, marked = 12, [100, 2000, 3001]
+    with tq.GpuState(tq.FP64) as g:
+        g.set_option(tq.OPT_EXACT, 0)
+        g.init_basis(n, 0)
+        g.apply_ops([tq.h(q) for q in range(n)])
+        v = tq.RegisterView.fresh()
+        iters = O.lib().or_grover_iterations(1 << n, 3)
+        g.grover_run(v, marked, iters, materialized)
+        r = O.OracleRegister(n)
+        r.run(O.grover_ops(n, marked, materialized))
+        for s in list(marked) + [0, 77, 4095]:
+            re, im = g.amplitude(s)
+            if v.overlay:
+                re, im = (v.scale_re * re - v.scale_im * im) + v.bias_re, (v.scale_re * im + v.scale_im * re) + v.bias_im
+            pr = r.amplitude(s)
+            assert abs(re - pr[0]) < 1e-12 and abs(im - pr[1]) < 1e-12

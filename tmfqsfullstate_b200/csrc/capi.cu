@@ -602,9 +602,17 @@ S storage_sub(double t, S v) {
 	return (S)t - v;
 }
 
+// Materialised Grover iterations with the register's semantics, all at once.
+// closed = false (exact form): the means are computed here exactly as the
+// register would, and the device replays every iteration per amplitude with
+// its rounding (k_grover_temporal).  closed = true (fast forms): an unmarked
+// amplitude follows a <- t_k - a, so after K iterations it is
+// (-1)^K a_0 + S_K with S_K independent of the amplitude; the run becomes one
+// affine sweep, with S_K and the marked amplitudes carried in FP64 and rounded
+// once into the state.
 template <typename S>
 void grover_materialized_fused(tmfqs_gpu_state *h, tmfqs_register_view *view, const std::vector<uint64_t> &marked,
-                               uint64_t iters) {
+                               uint64_t iters, bool closed) {
 	const double N = (double)h->N;
 	uint64_t flip_from = 0;
 	if(!view->has_sum) {
@@ -618,14 +626,15 @@ void grover_materialized_fused(tmfqs_gpu_state *h, tmfqs_register_view *view, co
 		view->sum_im = sum.im;
 		flip_from = 1;
 	}
-	std::vector<S> vr(marked.size()), vi(marked.size());
+	std::vector<double> vr(marked.size()), vi(marked.size());
 	for(size_t q = 0; q < marked.size(); ++q) {
 		const auto a = read_amp(h, marked[q]);
-		vr[q] = (S)a.first;
-		vi[q] = (S)a.second;
+		vr[q] = a.first;
+		vi[q] = a.second;
 	}
 	std::vector<double> tm(2 * iters);
 	double sr = view->sum_re, si = view->sum_im;
+	double bre = 0.0, bim = 0.0, sign = 1.0;  // closed form: a_K = sign * a_0 + b
 	for(uint64_t k = 0; k < iters; ++k) {
 		if(k >= flip_from) {
 			for(size_t q = 0; q < marked.size(); ++q) {
@@ -643,26 +652,49 @@ void grover_materialized_fused(tmfqs_gpu_state *h, tmfqs_register_view *view, co
 		tm[2 * k] = 2.0 * mr;
 		tm[2 * k + 1] = 2.0 * mi;
 		for(size_t q = 0; q < marked.size(); ++q) {
-			vr[q] = storage_sub<S>(tm[2 * k], vr[q]);
-			vi[q] = storage_sub<S>(tm[2 * k + 1], vi[q]);
+			if(closed) {
+				vr[q] = tm[2 * k] - vr[q];
+				vi[q] = tm[2 * k + 1] - vi[q];
+			} else {
+				vr[q] = (double)storage_sub<S>(tm[2 * k], (S)vr[q]);
+				vi[q] = (double)storage_sub<S>(tm[2 * k + 1], (S)vi[q]);
+			}
 		}
+		bre = tm[2 * k] - bre;
+		bim = tm[2 * k + 1] - bim;
+		sign = -sign;
 	}
 	before_mutation(h);
-	const size_t tm_bytes = iters * 16, mk_bytes = marked.size() * 8;
+	if(closed) {
+		{
+			PassTimer timer(h, TMFQS_KT_GROVER, sweep_bytes(h));
+			tqb::launch_affine(ctx(h), h->precision, h->amps, h->n, sign, 0.0, bre, bim);
+		}
+		++h->stats.fused_passes;
+		view->sum_re = sr;
+		view->sum_im = si;
+		for(size_t q = 0; q < marked.size(); ++q) write_amp(h, marked[q], vr[q], vi[q]);
+		return;
+	}
+	// The means in the storage type: the device rounds them exactly as the
+	// per-iteration update `(S)t - v` above does.
+	std::vector<S> tms(2 * iters);
+	for(size_t i = 0; i < tms.size(); ++i) tms[i] = (S)tm[i];
+	const size_t tm_bytes = iters * 2 * sizeof(S), mk_bytes = marked.size() * 8;
 	const size_t off = (tm_bytes + 255) & ~size_t(255);
 	ensure_dev_small(h, off + mk_bytes);
 	check_cuda(cudaStreamSynchronize(h->stream), "grover staging sync");
-	check_cuda(cudaMemcpyAsync(h->dev_small, tm.data(), tm_bytes, cudaMemcpyHostToDevice, h->stream), "grover means upload");
+	check_cuda(cudaMemcpyAsync(h->dev_small, tms.data(), tm_bytes, cudaMemcpyHostToDevice, h->stream), "grover means upload");
 	check_cuda(cudaMemcpyAsync(static_cast<unsigned char *>(h->dev_small) + off, marked.data(), mk_bytes, cudaMemcpyHostToDevice, h->stream), "grover marked upload");
 	PassTimer timer(h, TMFQS_KT_GROVER, sweep_bytes(h));
-	tqb::launch_grover_temporal(ctx(h), h->precision, h->amps, h->n, static_cast<const double *>(h->dev_small), iters,
+	tqb::launch_grover_temporal(ctx(h), h->precision, h->amps, h->n, h->dev_small, iters,
 	                            reinterpret_cast<const uint64_t *>(static_cast<unsigned char *>(h->dev_small) + off),
 	                            (unsigned)marked.size(), flip_from);
 	check_cuda(cudaStreamSynchronize(h->stream), "grover sync");
 	++h->stats.fused_passes;
 	view->sum_re = sr;
 	view->sum_im = si;
-	for(size_t q = 0; q < marked.size(); ++q) h->cache[marked[q]] = {(double)vr[q], (double)vi[q]};
+	for(size_t q = 0; q < marked.size(); ++q) h->cache[marked[q]] = {vr[q], vi[q]};
 }
 
 // One phase flip with register semantics (quantum_register.cpp:405-420).
@@ -1408,8 +1440,9 @@ int tmfqs_gpu_grover_run(tmfqs_gpu_state *h, tmfqs_register_view *view, const ui
 		DeviceScope d(h);
 		if(iterations == 0) return;
 		if(materialized && h->opt_grover_fusion && !view->overlay) {
-			if(h->precision == TMFQS_FP64) grover_materialized_fused<double>(h, view, mk, iterations);
-			else grover_materialized_fused<float>(h, view, mk, iterations);
+			const bool closed = h->precision == TMFQS_FP32 || !h->opt_exact;
+			if(h->precision == TMFQS_FP64) grover_materialized_fused<double>(h, view, mk, iterations, closed);
+			else grover_materialized_fused<float>(h, view, mk, iterations, closed);
 			return;
 		}
 		for(uint64_t k = 0; k < iterations; ++k) {

@@ -500,12 +500,20 @@ __global__ void __launch_bounds__(kPermThreads) k_bit_perm(typename Vec2<R>::typ
 // ---------------------------------------------------------------------------
 // Temporal Grover pass.
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(256) k_grover_temporal(typename Vec2<R>::type *a, uint64_t N, const double2 *tm,
-                                                        uint64_t iters, uint64_t flip_from, const uint64_t *marked,
-                                                        unsigned nm) {
+// v <- t - v for one amplitude: exactly the rounded subtraction (complex64
+// uses one paired instruction, fma(v, -1, t) rounds once like t - v).
+__device__ __forceinline__ void grover_step(double2 &v, double2 t) {
+	v.x = rsub(t.x, v.x);
+	v.y = rsub(t.y, v.y);
+}
+__device__ __forceinline__ void grover_step(float2 &v, float2 t) { v = __ffma2_rn(v, make_float2(-1.0f, -1.0f), t); }
+
+// tm[k] = 2 * mean of iteration k, already rounded to the storage type.
+template <typename R, unsigned kPer>
+__global__ void __launch_bounds__(256) k_grover_temporal(typename Vec2<R>::type *a, uint64_t N,
+                                                        const typename Vec2<R>::type *tm, uint64_t iters,
+                                                        uint64_t flip_from, const uint64_t *marked, unsigned nm) {
 	typedef typename Vec2<R>::type V;
-	constexpr unsigned kPer = 4;
 	for(uint64_t i0 = gtid() * kPer; i0 < N; i0 += gstride() * kPer) {
 		V v[kPer];
 		bool mk[kPer];
@@ -521,27 +529,33 @@ __global__ void __launch_bounds__(256) k_grover_temporal(typename Vec2<R>::type 
 			anymk = anymk || mk[u];
 		}
 		if(!anymk) {
-			for(uint64_t k = 0; k < iters; ++k) {
-				const double2 t = tm[k];
-				const R tr = (R)t.x, ti = (R)t.y;
+			uint64_t k = 0;
+			// Four means per trip, loaded ahead of the dependent updates.
+			for(; k + 4 <= iters; k += 4) {
+				const V t0 = tm[k], t1 = tm[k + 1], t2 = tm[k + 2], t3 = tm[k + 3];
 #pragma unroll
 				for(unsigned u = 0; u < kPer; ++u) {
-					v[u].x = rsub(tr, v[u].x);
-					v[u].y = rsub(ti, v[u].y);
+					grover_step(v[u], t0);
+					grover_step(v[u], t1);
+					grover_step(v[u], t2);
+					grover_step(v[u], t3);
 				}
+			}
+			for(; k < iters; ++k) {
+				const V t = tm[k];
+#pragma unroll
+				for(unsigned u = 0; u < kPer; ++u) grover_step(v[u], t);
 			}
 		} else {
 			for(uint64_t k = 0; k < iters; ++k) {
-				const double2 t = tm[k];
-				const R tr = (R)t.x, ti = (R)t.y;
+				const V t = tm[k];
 #pragma unroll
 				for(unsigned u = 0; u < kPer; ++u) {
 					if(mk[u] && k >= flip_from) {
 						v[u].x = -v[u].x;
 						v[u].y = -v[u].y;
 					}
-					v[u].x = rsub(tr, v[u].x);
-					v[u].y = rsub(ti, v[u].y);
+					grover_step(v[u], t);
 				}
 			}
 		}
@@ -692,17 +706,21 @@ void launch_bit_permutation(const LaunchCtx &c, int prec, void *a, unsigned n,
 	else run_perm<float>(c, a, n, pairs);
 }
 
-void launch_grover_temporal(const LaunchCtx &c, int prec, void *a, unsigned n, const double *dev_two_means,
+void launch_grover_temporal(const LaunchCtx &c, int prec, void *a, unsigned n, const void *dev_two_means,
                             uint64_t iterations, const uint64_t *dev_marked, unsigned marked_count,
                             uint64_t flip_from) {
 	const uint64_t N = 1ull << n;
-	const uint64_t threads = (N + 3) / 4;
+	const unsigned per = prec == TMFQS_FP64 ? 4u : 8u;
+	const uint64_t threads = (N + per - 1) / per;
 	const uint64_t blocks = std::max<uint64_t>(1, std::min<uint64_t>((threads + 255) / 256, (uint64_t)c.num_sms * 8));
-	const double2 *tm = reinterpret_cast<const double2 *>(dev_two_means);
 	if(prec == TMFQS_FP64)
-		k_grover_temporal<double><<<(unsigned)blocks, 256, 0, c.stream>>>(static_cast<double2 *>(a), N, tm, iterations, flip_from, dev_marked, marked_count);
+		k_grover_temporal<double, 4><<<(unsigned)blocks, 256, 0, c.stream>>>(
+			static_cast<double2 *>(a), N, static_cast<const double2 *>(dev_two_means), iterations, flip_from, dev_marked,
+			marked_count);
 	else
-		k_grover_temporal<float><<<(unsigned)blocks, 256, 0, c.stream>>>(static_cast<float2 *>(a), N, tm, iterations, flip_from, dev_marked, marked_count);
+		k_grover_temporal<float, 8><<<(unsigned)blocks, 256, 0, c.stream>>>(
+			static_cast<float2 *>(a), N, static_cast<const float2 *>(dev_two_means), iterations, flip_from, dev_marked,
+			marked_count);
 	after_launch(c, "grover temporal");
 }
 

@@ -176,9 +176,10 @@ void launch_bit_permutation(const LaunchCtx &c, int prec, void *a, unsigned n,
 
 // Materialised Grover iterations as one temporal pass: for k in [0,K):
 // flip marked states, then a <- two_mean[k] - a (exact per-iteration ops).
+// two_mean holds complex values in the storage type (double2 / float2).
 // Marked states are flipped from iteration `flip_from` on (the first
 // iteration's flips may already have been applied when its mean was taken).
-void launch_grover_temporal(const LaunchCtx &c, int prec, void *a, unsigned n, const double *dev_two_means,
+void launch_grover_temporal(const LaunchCtx &c, int prec, void *a, unsigned n, const void *dev_two_means,
                             uint64_t iterations, const uint64_t *dev_marked, unsigned marked_count,
                             uint64_t flip_from);
 
