@@ -109,9 +109,8 @@ struct RadixSmem {
 	uint32_t *items;
 	V *tabs;          // in-stage phase tables
 	V *A;             // [nslots][2^lo]
-	double2 *Bbase;   // [nslots][2^(K-lo)]
-	V *Bt;            // [nslots][2^(K-lo)], per tile
-	double2 *Ot;      // [nslots] outer phase x scale of the current tile
+	V *B;             // [nslots][2^(K-lo)]
+	V *Ot[2];         // [nslots] outer phase x scale of the current / next tile
 };
 
 template <typename V>
@@ -311,15 +310,15 @@ __device__ __noinline__ V thread_terms(V f, const RadixTerm *terms, unsigned fir
 // Multiplies v[r] by the product of the active factors of a slot group:
 // factor 0 for every r (if bit 0 of mask), factor i+1 for r with bit i.
 template <typename V, int RB>
-__device__ __forceinline__ void apply_factors(V (&v)[1 << RB], const RadixSmem<V> &sh, unsigned slot0, unsigned mask,
-                                              unsigned ia, unsigned ib, unsigned lo, unsigned nb, const RadixTerm *terms,
+__device__ __forceinline__ void apply_factors(V (&v)[1 << RB], const RadixSmem<V> &sh, const V *ot, unsigned slot0,
+                                              unsigned mask, unsigned ia, unsigned ib, unsigned lo, unsigned nb, const RadixTerm *terms,
                                               unsigned xfirst, unsigned xcount, unsigned jt, uint64_t base) {
 	V f[RB + 1];
 	unsigned s = slot0;
 #pragma unroll
 	for(int i = 0; i <= RB; ++i) {
 		if((mask >> i) & 1u) {
-			f[i] = vmul(sh.A[(s << lo) + ia], sh.Bt[s * nb + ib]);
+			f[i] = vmul(vmul(sh.A[(s << lo) + ia], sh.B[s * nb + ib]), ot[s]);
 			if(i == 0 && xcount) f[0] = thread_terms(f[0], terms, xfirst, xcount, jt, base);
 			++s;
 		} else {
@@ -355,7 +354,7 @@ namespace {
 template <typename R, int RB>
 __global__ void __launch_bounds__(kRadixThreads, 1)
 	k_radix(typename Vec2<R>::type *a, RadixGeom g, const unsigned char *prog, size_t off_stages, size_t off_items,
-	        size_t off_tabs, size_t off_slots, size_t off_terms) {
+	        size_t off_tabs, size_t off_slots, size_t off_terms, const typename Vec2<R>::type *otab, unsigned ot_stride) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const unsigned T = 1u << g.K;
@@ -381,9 +380,9 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 	sh.items = reinterpret_cast<uint32_t *>(take(sizeof(uint32_t) * g.nitems));
 	sh.tabs = reinterpret_cast<V *>(take(sizeof(V) * g.ntab));
 	sh.A = reinterpret_cast<V *>(take(sizeof(V) * ((size_t)g.nslots << g.lo)));
-	sh.Bbase = reinterpret_cast<double2 *>(take(sizeof(double2) * g.nslots * nb));
-	sh.Bt = reinterpret_cast<V *>(take(sizeof(V) * g.nslots * nb));
-	sh.Ot = reinterpret_cast<double2 *>(take(sizeof(double2) * g.nslots));
+	sh.B = reinterpret_cast<V *>(take(sizeof(V) * g.nslots * nb));
+	sh.Ot[0] = reinterpret_cast<V *>(take(sizeof(V) * ot_stride));
+	sh.Ot[1] = reinterpret_cast<V *>(take(sizeof(V) * ot_stride));
 
 	const unsigned tid = threadIdx.x, nthr = blockDim.x;
 	const unsigned lowmask = (1u << g.m) - 1u;
@@ -401,18 +400,22 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 	};
 	// Granules of 16 bytes: one complex128 or two complex64 amplitudes.
 	constexpr unsigned per16 = 16 / sizeof(V);
-	auto prefetch = [&](uint64_t o, uint64_t base, V *dst) {
+	// A tile's amplitudes and its row of outer phases (ot_stride values, a
+	// multiple of 16 bytes) arrive in one copy group.
+	auto prefetch = [&](uint64_t o, uint64_t base, V *dst, V *odst) {
 		if(o < g.ntiles) {
 			for(unsigned q = tid; q < T / per16; q += nthr) {
 				const unsigned j = q * per16;
 				cp_async16(dst + rswz<V>(j), a + (base | scatter(j)));
 			}
+			for(unsigned q = tid; q < ot_stride / per16; q += nthr)
+				cp_async16(odst + q * per16, otab + o * ot_stride + q * per16);
 		}
 		cp_async_commit();
 	};
 	// The first tile's copy starts before the tables are built.
 	uint64_t cbase = tile_base(blockIdx.x);
-	prefetch(blockIdx.x, cbase, sh.buf[0]);
+	prefetch(blockIdx.x, cbase, sh.buf[0], sh.Ot[0]);
 
 	for(unsigned k = tid; k < g.nstages; k += nthr) sh.stages[k] = gstages[k];
 	for(unsigned k = tid; k < g.nitems; k += nthr) sh.items[k] = gitems[k];
@@ -435,13 +438,7 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 		double sv, cv;
 		sincos(ang, &sv, &cv);
 		if(is_a) sh.A[(s << g.lo) + x] = to_v<V>(make_double2(cv, sv));
-		else sh.Bbase[s * nb + x] = make_double2(cv, sv);
-	}
-	if(tid < g.nslots) {
-		const RadixSlot sl = gslots[tid];
-		double sv, cv;
-		sincos(slot_outer_angle(sl, gterms, cbase), &sv, &cv);
-		sh.Ot[tid] = make_double2(cv * sl.scale, sv * sl.scale);
+		else sh.B[s * nb + x] = to_v<V>(make_double2(cv, sv));
 	}
 	__syncthreads();
 
@@ -449,12 +446,8 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 	for(uint64_t o = blockIdx.x; o < g.ntiles; o += gridDim.x, cur ^= 1u) {
 		const uint64_t next = o + gridDim.x;
 		const uint64_t nbase = next < g.ntiles ? tile_base(next) : cbase;
-		prefetch(next, nbase, sh.buf[cur ^ 1u]);
-		// This tile's factor tables: local phase times the tile's outer phase.
-		for(unsigned t = tid; t < g.nslots * nb; t += nthr) {
-			const double2 b = sh.Bbase[t], c = sh.Ot[t / nb];
-			sh.Bt[t] = to_v<V>(make_double2(fma(b.x, c.x, -(b.y * c.y)), fma(b.x, c.y, b.y * c.x)));
-		}
+		prefetch(next, nbase, sh.buf[cur ^ 1u], sh.Ot[cur ^ 1u]);
+		const V *ot = sh.Ot[cur];
 		cp_async_wait1();
 		__syncthreads();
 		V *tile = sh.buf[cur];
@@ -478,7 +471,7 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 #pragma unroll
 			for(int r = 0; r < (1 << RB); ++r) v[r] = tile[addr(r)];
 			const unsigned ia = jt & ((1u << g.lo) - 1u), ib = jt >> g.lo;
-			if(S.pre_mask) apply_factors<V, RB>(v, sh, S.pre_slot, S.pre_mask, ia, ib, g.lo, nb, gterms, 0, 0, jt, cbase);
+			if(S.pre_mask) apply_factors<V, RB>(v, sh, ot, S.pre_slot, S.pre_mask, ia, ib, g.lo, nb, gterms, 0, 0, jt, cbase);
 			for(unsigned k = S.first; k < S.first + S.count; ++k) {
 				const uint32_t it = sh.items[k];
 				const unsigned kind = it & 0xffu, b = (it >> 8) & 0xffu;
@@ -493,16 +486,9 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 				}
 			}
 			if(S.post_mask)
-				apply_factors<V, RB>(v, sh, S.post_slot, S.post_mask, ia, ib, g.lo, nb, gterms, S.post_xfirst, S.post_xcount, jt,
+				apply_factors<V, RB>(v, sh, ot, S.post_slot, S.post_mask, ia, ib, g.lo, nb, gterms, S.post_xfirst, S.post_xcount, jt,
 				                     cbase);
 			const bool last = st + 1 == g.nstages;
-			if(last && tid < g.nslots) {
-				// Next tile's outer phases (this tile's tables are already built).
-				const RadixSlot sl = gslots[tid];
-				double sv, cv;
-				sincos(slot_outer_angle(sl, gterms, nbase), &sv, &cv);
-				sh.Ot[tid] = make_double2(cv * sl.scale, sv * sl.scale);
-			}
 			if(last && S.direct) {
 				// Lanes run along the low address bits: coalesced stores.
 				const uint64_t gt = cbase | scatter(jt);
@@ -540,6 +526,24 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 }  // namespace
 
 namespace {
+
+// The outer-bit phase of every slot for every tile (times the slot's scale),
+// rounded once to the storage type: otab[o * stride + s].
+template <typename R>
+__global__ void __launch_bounds__(256) k_outer_table(typename Vec2<R>::type *otab, unsigned stride, RadixGeom g,
+                                                    const RadixSlot *slots, const RadixTerm *terms) {
+	typedef typename Vec2<R>::type V;
+	for(uint64_t e = gtid(); e < g.ntiles * g.nslots; e += gstride()) {
+		const uint64_t o = e / g.nslots;
+		const unsigned s = (unsigned)(e - o * g.nslots);
+		uint64_t base = o;
+		for(unsigned i = 0; i < g.K; ++i) base = insert0(base, g.lpos[i]);
+		const RadixSlot sl = slots[s];
+		double sv, cv;
+		sincos(slot_outer_angle(sl, terms, base), &sv, &cv);
+		otab[o * stride + s] = to_v<V>(make_double2(cv * sl.scale, sv * sl.scale));
+	}
+}
 
 struct BitRef {
 	bool local;
@@ -829,9 +833,10 @@ bool build_radix_program(const FusedPass &pass, unsigned K, size_t vbytes, Radix
 size_t radix_smem_bytes(size_t vbytes, const RadixGeom &g) {
 	auto a16 = [](size_t b) { return (b + 15) & ~size_t(15); };
 	const size_t nb = size_t(1) << (g.K - g.lo);
+	const size_t stride = (g.nslots * vbytes + 15) / 16 * 16;
 	return 2 * a16(vbytes << g.K) + a16(sizeof(uint64_t) << (g.K - g.m)) + a16(sizeof(RadixStage) * g.nstages) +
 	       a16(sizeof(uint32_t) * g.nitems) + a16(vbytes * g.ntab) + a16(vbytes * ((size_t)g.nslots << g.lo)) +
-	       a16(sizeof(double2) * g.nslots * nb) + a16(vbytes * g.nslots * nb) + a16(sizeof(double2) * g.nslots);
+	       a16(vbytes * g.nslots * nb) + 2 * a16(stride);
 }
 
 template <typename R, int RB>
@@ -854,7 +859,10 @@ bool run_radix(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	const size_t o_st = 0, o_it = o_st + a256(P.stages.size() * sizeof(RadixStage)),
 	             o_tb = o_it + a256(P.items.size() * sizeof(uint32_t)), o_sl = o_tb + a256(P.tabs.size() * sizeof(double2)),
 	             o_tm = o_sl + a256(P.slots.size() * sizeof(RadixSlot)),
-	             need = std::max<size_t>(256, o_tm + a256(P.terms.size() * sizeof(RadixTerm)));
+	             o_ot = o_tm + a256(P.terms.size() * sizeof(RadixTerm));
+	// Per-tile outer phases: ot_stride storage values per tile (16-byte rows).
+	const unsigned ot_stride = (unsigned)((P.g.nslots * sizeof(V) + 15) / 16 * 16 / sizeof(V));
+	const size_t upload = std::max<size_t>(256, o_ot), need = o_ot + a256(P.g.ntiles * ot_stride * sizeof(V));
 	if(need > dev_prog_bytes) {
 		if(dev_prog) {
 			check_cuda(cudaStreamSynchronize(c.stream), "radix program sync");
@@ -862,27 +870,38 @@ bool run_radix(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 		}
 		dev_prog = nullptr;
 		dev_prog_bytes = 0;
-		if(cudaMalloc(&dev_prog, need * 2) != cudaSuccess) {
+		const size_t want = need + need / 8;
+		if(cudaMalloc(&dev_prog, want) != cudaSuccess) {
 			cudaGetLastError();
 			fail(TMFQS_ERR_NOMEM, "radix pass program allocation failed");
 		}
-		dev_prog_bytes = need * 2;
+		dev_prog_bytes = want;
 	}
-	std::vector<unsigned char> host(need, 0);
+	std::vector<unsigned char> host(upload, 0);
 	std::memcpy(host.data() + o_st, P.stages.data(), P.stages.size() * sizeof(RadixStage));
 	std::memcpy(host.data() + o_it, P.items.data(), P.items.size() * sizeof(uint32_t));
 	std::memcpy(host.data() + o_tb, P.tabs.data(), P.tabs.size() * sizeof(double2));
 	std::memcpy(host.data() + o_sl, P.slots.data(), P.slots.size() * sizeof(RadixSlot));
 	std::memcpy(host.data() + o_tm, P.terms.data(), P.terms.size() * sizeof(RadixTerm));
-	check_cuda(cudaMemcpyAsync(dev_prog, host.data(), need, cudaMemcpyHostToDevice, c.stream), "radix program upload");
+	check_cuda(cudaMemcpyAsync(dev_prog, host.data(), upload, cudaMemcpyHostToDevice, c.stream), "radix program upload");
 	check_cuda(cudaStreamSynchronize(c.stream), "radix program upload sync");
+	unsigned char *pbase = static_cast<unsigned char *>(dev_prog);
+	V *otab = reinterpret_cast<V *>(pbase + o_ot);
+	if(P.g.nslots) {
+		const uint64_t work = P.g.ntiles * P.g.nslots;
+		const unsigned blocks = (unsigned)std::min<uint64_t>((work + 255) / 256, (uint64_t)c.num_sms * 8);
+		k_outer_table<R><<<blocks, 256, 0, c.stream>>>(otab, ot_stride, P.g, reinterpret_cast<const RadixSlot *>(pbase + o_sl),
+		                                               reinterpret_cast<const RadixTerm *>(pbase + o_tm));
+		check_cuda(cudaGetLastError(), "radix outer phases");
+		if(c.launches) ++*c.launches;
+	}
 
 	const unsigned threads = 1u << (K - RB);
 	check_cuda(cudaFuncSetAttribute(k_radix<R, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "radix smem");
 	const uint64_t grid = std::min<uint64_t>(P.g.ntiles, (uint64_t)c.num_sms);
 	k_radix<R, RB><<<(unsigned)grid, threads, smem, c.stream>>>(static_cast<V *>(a), P.g,
 	                                                           static_cast<const unsigned char *>(dev_prog), o_st, o_it,
-	                                                           o_tb, o_sl, o_tm);
+	                                                           o_tb, o_sl, o_tm, otab, ot_stride);
 	check_cuda(cudaGetLastError(), "radix pass");
 	if(c.launches) ++*c.launches;
 	return true;
