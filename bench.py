@@ -367,6 +367,8 @@ def run_qft32(tq, torch, device, peak):
             fid, rel = _compare(torch, g128.tensor(), g64.tensor())
             res["fidelity_c64_vs_c128"] = fid
             res["rel_l2_c64_vs_c128"] = rel
+            # experiment::compareStates on the device (reference semantics, exact sums).
+            res["compare_states_c64_vs_c128"] = g128.compare(g64)
             res["speedup_c64_vs_c128_plain"] = res["complex128_plain"]["ms_per_qft"] / res["complex64_radix"]["ms_per_qft"]
             if inp == "pattern":
                 res["max_abs_err_vs_analytic"] = {"complex64": _pattern_error(torch, g64.tensor(), n, m),

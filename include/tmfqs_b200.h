@@ -88,6 +88,18 @@ typedef struct {
 	double bias_re, bias_im;
 } tmfqs_register_view;
 
+/* experiment::StateComparison (experiment/comparison.h:19-28), field for field. */
+typedef struct {
+	int bitwise_equal;
+	double max_abs_amplitude_error;
+	double max_abs_component_error;
+	double rmse_amplitude;
+	double rel_l2;
+	double max_abs_probability_error;
+	double total_probability_diff;
+	uint64_t worst_state;
+} tmfqs_state_comparison;
+
 /* Counters of the work a handle has issued (for benchmarks and tests). */
 typedef struct {
 	uint64_t kernel_launches;   /* kernels launched by this handle */
@@ -253,6 +265,12 @@ TMFQS_API int tmfqs_sample_static(const void *device_amps, int precision, unsign
 TMFQS_API int tmfqs_gpu_adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count,
                                          const uint64_t *obs_masks, const double *obs_weights, unsigned obs_terms,
                                          size_t checkpoint_every, double *expectation, double *grads);
+/* experiment::compareStates(reference, candidate), comparison.cpp:12-62, on
+ * two device states of the same qubit count (either precision, same device):
+ * every field equals the reference's, bit for bit -- its left-to-right FP64
+ * sums are replayed exactly.  Compares the stored amplitudes (a register's
+ * lazy overlay is not applied). */
+TMFQS_API int tmfqs_gpu_compare(tmfqs_gpu_state *reference, tmfqs_gpu_state *candidate, tmfqs_state_comparison *out);
 /* endOperationBatch, i_state_backend.h:163: waits for all queued work. */
 TMFQS_API int tmfqs_gpu_sync(tmfqs_gpu_state *h);
 

@@ -166,6 +166,7 @@ def ref() -> ctypes.CDLL:
             "ref_grover_iterations": (ctypes.c_uint, [ctypes.c_uint64, ctypes.c_size_t]),
             "ref_mt_unit": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_size_t, dp]),
             "ref_compare": (ctypes.c_int, [ctypes.c_uint, dp, dp, dp, dp, u64p, ctypes.POINTER(ctypes.c_int)]),
+            "ref_compare_full": (ctypes.c_int, [ctypes.c_uint, dp, dp, dp, u64p, ctypes.POINTER(ctypes.c_int)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(R, name)
@@ -508,6 +509,24 @@ def ref_compare(n, ref_amps, got_amps):
     if rc:
         raise RuntimeError(ref().ref_last_error().decode())
     return rl2.value, mx.value, worst.value, bool(bw.value)
+
+
+COMPARE_FIELDS = ("bitwise_equal", "max_abs_amplitude_error", "max_abs_component_error", "rmse_amplitude", "rel_l2",
+                  "max_abs_probability_error", "total_probability_diff", "worst_state")
+
+
+def ref_compare_full(n, ref_amps, got_amps) -> dict:
+    """Every field of the reference's experiment::compareStates (comparison.cpp:12-62)."""
+    out = np.zeros(6)
+    worst, bw = ctypes.c_uint64(), ctypes.c_int()
+    a = np.ascontiguousarray(ref_amps, dtype=np.float64)
+    b = np.ascontiguousarray(got_amps, dtype=np.float64)
+    rc = ref().ref_compare_full(n, dptr(a), dptr(b), dptr(out), ctypes.byref(worst), ctypes.byref(bw))
+    if rc:
+        raise RuntimeError(ref().ref_last_error().decode())
+    return {"bitwise_equal": bool(bw.value), "max_abs_amplitude_error": out[0], "max_abs_component_error": out[1],
+            "rmse_amplitude": out[2], "rel_l2": out[3], "max_abs_probability_error": out[4],
+            "total_probability_diff": out[5], "worst_state": worst.value}
 
 
 def rel_l2(ref_amps: np.ndarray, got_amps: np.ndarray) -> float:

@@ -330,6 +330,29 @@ REF_API int ref_mt_unit(std::uint32_t seed, size_t k, double *out) {
 }
 
 // experiment::compareStates between two interleaved amplitude vectors.
+// All of experiment::compareStates: out = {maxAbsAmplitudeError,
+// maxAbsComponentError, rmseAmplitude, relL2, maxAbsProbabilityError,
+// totalProbabilityDiff}.
+REF_API int ref_compare_full(unsigned n, const double *ref_amps, const double *got_amps, double *out,
+                             std::uint64_t *worst, int *bitwise) {
+	return guarded([&] {
+		const size_t len = static_cast<size_t>(2) << n;
+		tmfqs::state::StateValidation v;
+		v.normalization = tmfqs::state::NormalizationPolicy::AllowUnnormalized;
+		const auto a = tmfqs::state::QuantumState::fromAmplitudes(n, tmfqs::AmplitudesVector(ref_amps, ref_amps + len), v);
+		const auto b = tmfqs::state::QuantumState::fromAmplitudes(n, tmfqs::AmplitudesVector(got_amps, got_amps + len), v);
+		const tmfqs::experiment::StateComparison c = tmfqs::experiment::compareStates(a, b);
+		out[0] = c.maxAbsAmplitudeError;
+		out[1] = c.maxAbsComponentError;
+		out[2] = c.rmseAmplitude;
+		out[3] = c.relL2;
+		out[4] = c.maxAbsProbabilityError;
+		out[5] = c.totalProbabilityDiff;
+		*worst = c.worstState;
+		*bitwise = c.bitwiseEqual ? 1 : 0;
+	});
+}
+
 REF_API int ref_compare(unsigned n, const double *ref_amps, const double *got_amps, double *rel_l2,
                         double *max_abs, std::uint64_t *worst, int *bitwise) {
 	return guarded([&] {

@@ -106,6 +106,13 @@ OPT_EXACT = 4
 OPT_RADIX = 5
 
 
+class StateComparison(ctypes.Structure):
+    _fields_ = [("bitwise_equal", ctypes.c_int), ("max_abs_amplitude_error", ctypes.c_double),
+                ("max_abs_component_error", ctypes.c_double), ("rmse_amplitude", ctypes.c_double),
+                ("rel_l2", ctypes.c_double), ("max_abs_probability_error", ctypes.c_double),
+                ("total_probability_diff", ctypes.c_double), ("worst_state", ctypes.c_uint64)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("kernel_launches", ctypes.c_uint64),
@@ -160,6 +167,7 @@ SIGNATURES = {
     "tmfqs_gpu_grover_run": [_H, ctypes.POINTER(RegisterView), _U64P, ctypes.c_size_t, _U64, ctypes.c_int],
     "tmfqs_gpu_adjoint_gradient": [_H, ctypes.POINTER(Op), ctypes.c_size_t, _U64P, _DP, _UI, ctypes.c_size_t, _DP,
                                    _DP],
+    "tmfqs_gpu_compare": [_H, _H, ctypes.POINTER(StateComparison)],
     "tmfqs_gpu_sync": [_H],
     "tmfqs_gpu_stats": [_H, ctypes.POINTER(Stats)],
     "tmfqs_gpu_reset_stats": [_H],
@@ -501,6 +509,14 @@ class GpuState:
         _check(lib().tmfqs_gpu_adjoint_gradient(self._h, arr, len(ops), m.ctypes.data_as(_U64P), _dptr(w), len(m),
                                                 checkpoint_every, ctypes.byref(e), _dptr(grads)))
         return e.value, grads[:nparams]
+
+    def compare(self, candidate: "GpuState") -> dict:
+        """experiment::compareStates(self, candidate) on the device, field for field."""
+        out = StateComparison()
+        _check(lib().tmfqs_gpu_compare(self._h, candidate._h, ctypes.byref(out)))
+        d = {f: getattr(out, f) for f, _ in StateComparison._fields_}
+        d["bitwise_equal"] = bool(d["bitwise_equal"])
+        return d
 
     def tensor(self):
         """A torch tensor viewing the handle's device state (interleaved re, im;

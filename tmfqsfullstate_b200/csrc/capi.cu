@@ -1475,6 +1475,37 @@ int tmfqs_gpu_adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t c
 	});
 }
 
+int tmfqs_gpu_compare(tmfqs_gpu_state *ref, tmfqs_gpu_state *got, tmfqs_state_comparison *out) {
+	return guarded([&] {
+		ensure_initialized(ref, "compare");
+		ensure_initialized(got, "compare");
+		if(!out) fail(TMFQS_ERR_INVALID_ARGUMENT, "null comparison output");
+		if(ref->N != got->N) fail(TMFQS_ERR_INVALID_ARGUMENT, "Compared states must have the same state count");
+		if(ref->device != got->device) fail(TMFQS_ERR_INVALID_ARGUMENT, "compare: states on different devices");
+		DeviceScope d(ref);
+		flush_dirty(got);
+		check_cuda(cudaStreamSynchronize(got->stream), "compare sync");
+		flush_dirty(ref);
+		tqb::CompareReport r{};
+		tqb::launch_compare(ctx(ref), ref->precision, ref->amps, got->precision, got->amps, ref->N, r);
+		const tqb::Overlay none;
+		const double ref_sq = tqb::seq_replay(ref->precision, ref->amps, ref->N, tqb::kTermProb, none, false, 0.0, ref->seq,
+		                                      ref->stream, ref->num_sms, &ref->stats.kernel_launches).value;
+		const double got_sq = tqb::seq_replay(got->precision, got->amps, got->N, tqb::kTermProb, none, false, 0.0, got->seq,
+		                                      got->stream, got->num_sms, &got->stats.kernel_launches).value;
+		const double diff_sq = tqb::seq_diff_norm(ref->precision, ref->amps, got->precision, got->amps, ref->N, ref->seq,
+		                                          ref->stream, ref->num_sms, &ref->stats.kernel_launches);
+		out->bitwise_equal = r.bitwise_equal ? 1 : 0;
+		out->max_abs_amplitude_error = r.max_abs_amplitude_error;
+		out->max_abs_component_error = r.max_abs_component_error;
+		out->rmse_amplitude = std::sqrt(diff_sq / static_cast<double>(ref->N));
+		out->rel_l2 = ref_sq == 0.0 ? 0.0 : std::sqrt(diff_sq / ref_sq);
+		out->max_abs_probability_error = r.max_abs_probability_error;
+		out->total_probability_diff = std::abs(got_sq - ref_sq);
+		out->worst_state = r.worst_state;
+	});
+}
+
 int tmfqs_gpu_sync(tmfqs_gpu_state *h) {
 	return guarded([&] {
 		require_handle(h);

@@ -55,6 +55,10 @@ struct SeqResult {
 SeqResult seq_replay(int precision, const void *amps, uint64_t N, TermKind kind, const Overlay &ov, bool stop,
                      double rnd, SeqScratch &scratch, cudaStream_t stream, int num_sms, uint64_t *launches);
 void seq_scratch_free(SeqScratch &scratch);
+// The reference's left-to-right sum over j of |got_j - ref_j|^2
+// (experiment::compareStates), exactly.  Synchronises.
+double seq_diff_norm(int prec_ref, const void *ref, int prec_got, const void *got, uint64_t N, SeqScratch &scratch,
+                     cudaStream_t stream, int num_sms, uint64_t *launches);
 // sampleMeasurement over a caller-owned device state, using the library's
 // fixed device scratch instead of allocating (tmfqs_sample_static).
 SeqResult seq_sample_static(int precision, const void *amps, unsigned num_qubits, double rnd, cudaStream_t stream);
@@ -168,6 +172,17 @@ unsigned launch_obs_apply(const LaunchCtx &c, int prec, const void *psi, void *l
 // then the run's inverse on lambda (and on psi if asked); returns the blocks.
 unsigned launch_grad_run(const LaunchCtx &c, int prec, void *lam, void *psi, unsigned n, const DiagEntry *entries,
                          unsigned count, bool uncompute_psi, double *dev_partials);
+
+// ---------------------------------------------------------------------------
+// Device compareStates (compare.cu): the order-independent fields.
+// ---------------------------------------------------------------------------
+struct CompareReport {
+	bool bitwise_equal;
+	double max_abs_amplitude_error, max_abs_component_error, max_abs_probability_error;
+	uint64_t worst_state;
+};
+void launch_compare(const LaunchCtx &c, int prec_ref, const void *ref, int prec_got, const void *got, uint64_t N,
+                    CompareReport &out);
 
 // Involutive permutation of bit positions (disjoint transpositions), as one
 // in-place pass: amplitude x moves to perm(x).  pairs[i] = (p, q) bit positions.

@@ -81,6 +81,23 @@ struct TermF {
 	}
 };
 
+// Squared distance of two states at j, as experiment::compareStates forms it
+// (comparison.cpp:29-38): the candidate minus the reference, per component,
+// in double.
+template <typename RA, typename RB>
+struct TermDiff {
+	const typename Vec2<RA>::type *ref;
+	const typename Vec2<RB>::type *got;
+	uint64_t N;
+	__device__ __forceinline__ double operator()(uint64_t j) const {
+		if(j >= N) return 0.0;
+		const auto r = ref[j];
+		const auto g = got[j];
+		const double dr = rsub((double)g.x, (double)r.x), di = rsub((double)g.y, (double)r.y);
+		return radd(rmul(dr, dr), rmul(di, di));
+	}
+};
+
 __device__ __forceinline__ tq::DD shfl_dd(tq::DD v, int src) {
 	return tq::DD{__shfl_sync(FULL, v.hi, src), __shfl_sync(FULL, v.lo, src)};
 }
@@ -489,11 +506,9 @@ __global__ void __launch_bounds__(32) k_seq_walk(F term, uint64_t N, uint64_t nt
 	if((threadIdx.x & 31u) == 0) *out = WalkOut{st.done ? st.answer : N, st.C, st.err, 0};
 }
 
-template <typename R, int KIND>
-SeqResult run_engine(const void *amps, uint64_t N, const Overlay &ov, bool stop, double rnd, SeqScratch &s,
-                     cudaStream_t stream, int num_sms, uint64_t *launches) {
-	constexpr bool SIGNED = KIND != kTermProb;
-	TermF<R, KIND> term{static_cast<const typename Vec2<R>::type *>(amps), N, ov.active ? 1 : 0, ov.sre, ov.sim, ov.bre, ov.bim};
+template <class Term, bool SIGNED>
+SeqResult run_engine_term(const Term &term, uint64_t N, bool stop, double rnd, SeqScratch &s, cudaStream_t stream,
+                          int num_sms, uint64_t *launches) {
 	const uint64_t ntiles = s.tiles, ngroups = s.groups;
 	auto *ta = static_cast<TileA *>(s.tile_a);
 	auto *tp = static_cast<TilePre *>(s.tile_pre);
@@ -504,13 +519,13 @@ SeqResult run_engine(const void *amps, uint64_t N, const Overlay &ov, bool stop,
 	auto *wo = static_cast<WalkOut *>(s.walk_out);
 	const unsigned gridA = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((ntiles + kWarpsA - 1) / kWarpsA, (uint64_t)num_sms * 6));
 	const unsigned gridG = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((ngroups + 7) / 8, (uint64_t)num_sms * 8));
-	k_seq_a<TermF<R, KIND>, SIGNED><<<gridA, kWarpsA * 32, 0, stream>>>(term, ntiles, ta);
+	k_seq_a<Term, SIGNED><<<gridA, kWarpsA * 32, 0, stream>>>(term, ntiles, ta);
 	k_seq_groups<<<gridG, 256, 0, stream>>>(ta, ntiles, ngroups, tp, ga);
 	k_seq_top<<<1, 1024, 0, stream>>>(ga, ngroups, gp);
-	k_seq_b<TermF<R, KIND>, SIGNED><<<gridA, kWarpsA * 32, 0, stream>>>(term, N, ntiles, ta, tp, gp, tb);
+	k_seq_b<Term, SIGNED><<<gridA, kWarpsA * 32, 0, stream>>>(term, N, ntiles, ta, tp, gp, tb);
 	k_seq_groupb<<<gridG, 256, 0, stream>>>(tb, ntiles, ngroups, gb);
-	if(stop) k_seq_walk<TermF<R, KIND>, true><<<1, 32, 0, stream>>>(term, N, ntiles, ngroups, tb, gb, rnd, wo);
-	else k_seq_walk<TermF<R, KIND>, false><<<1, 32, 0, stream>>>(term, N, ntiles, ngroups, tb, gb, rnd, wo);
+	if(stop) k_seq_walk<Term, true><<<1, 32, 0, stream>>>(term, N, ntiles, ngroups, tb, gb, rnd, wo);
+	else k_seq_walk<Term, false><<<1, 32, 0, stream>>>(term, N, ntiles, ngroups, tb, gb, rnd, wo);
 	check_cuda(cudaGetLastError(), "exact reduction");
 	if(launches) *launches += 6;
 	check_cuda(cudaMemcpyAsync(s.host_out, wo, sizeof(WalkOut), cudaMemcpyDeviceToHost, stream), "reduction readback");
@@ -518,6 +533,13 @@ SeqResult run_engine(const void *amps, uint64_t N, const Overlay &ov, bool stop,
 	const WalkOut r = *static_cast<WalkOut *>(s.host_out);
 	if(r.error) fail(TMFQS_ERR_RUNTIME, "exact reduction invariant violated (code " + std::to_string(r.error) + ")");
 	return SeqResult{r.index, r.value};
+}
+
+template <typename R, int KIND>
+SeqResult run_engine(const void *amps, uint64_t N, const Overlay &ov, bool stop, double rnd, SeqScratch &s,
+                     cudaStream_t stream, int num_sms, uint64_t *launches) {
+	TermF<R, KIND> term{static_cast<const typename Vec2<R>::type *>(amps), N, ov.active ? 1 : 0, ov.sre, ov.sim, ov.bre, ov.bim};
+	return run_engine_term<TermF<R, KIND>, KIND != kTermProb>(term, N, stop, rnd, s, stream, num_sms, launches);
 }
 
 void ensure_scratch(SeqScratch &s, uint64_t N) {
@@ -653,6 +675,19 @@ void seq_scratch_free(SeqScratch &s) {
 	if(s.base) cudaFree(s.base);
 	if(s.host_out) cudaFreeHost(s.host_out);
 	s = SeqScratch{};
+}
+
+double seq_diff_norm(int prec_ref, const void *ref, int prec_got, const void *got, uint64_t N, SeqScratch &scratch,
+                     cudaStream_t stream, int num_sms, uint64_t *launches) {
+	ensure_scratch(scratch, N);
+	auto run = [&](auto term) { return run_engine_term<decltype(term), false>(term, N, false, 0.0, scratch, stream, num_sms, launches).value; };
+	if(prec_ref == TMFQS_FP64 && prec_got == TMFQS_FP64)
+		return run(TermDiff<double, double>{static_cast<const double2 *>(ref), static_cast<const double2 *>(got), N});
+	if(prec_ref == TMFQS_FP64)
+		return run(TermDiff<double, float>{static_cast<const double2 *>(ref), static_cast<const float2 *>(got), N});
+	if(prec_got == TMFQS_FP64)
+		return run(TermDiff<float, double>{static_cast<const float2 *>(ref), static_cast<const double2 *>(got), N});
+	return run(TermDiff<float, float>{static_cast<const float2 *>(ref), static_cast<const float2 *>(got), N});
 }
 
 SeqResult seq_replay(int precision, const void *amps, uint64_t N, TermKind kind, const Overlay &ov, bool stop,
