@@ -162,19 +162,11 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 								const int l = cloc[e];
 								const R pr = (R)ph.x, pi = (R)ph.y;
 								// An entry whose local bit is clear leaves the value as it is
-								// (a product with (1, 0) could turn a -0 component into +0).
+								// (a product with (1, 0) could turn a -0 component into +0);
+								// the products run under the condition, not through a select.
 								const bool on0 = l < 0 || ((j01 >> l) & 1u), on1 = l < 0 || ((j11 >> l) & 1u);
-								R s0 = r0, t0 = i0, s1 = r1, t1 = i1;
-								cmul_ref(pr, pi, s0, t0);
-								cmul_ref(pr, pi, s1, t1);
-								if(on0) {
-									r0 = s0;
-									i0 = t0;
-								}
-								if(on1) {
-									r1 = s1;
-									i1 = t1;
-								}
+								if(on0) cmul_ref(pr, pi, r0, i0);
+								if(on1) cmul_ref(pr, pi, r1, i1);
 							}
 							if(c0) {
 								y0.x = r0;
