@@ -36,6 +36,10 @@ between steps.
           12867 iterations, lazy and materialised diffusion, complex64 (8 GiB)
           and complex128 (16 GiB): per-iteration time and the marked-state
           probability error of complex64.
+  block_gate a dense 5-qubit gate (random unitary, a fused 32 x 32 block) on a
+          30-qubit complex64 state: the 3xTF32 tensor-core GEMM kernel beside
+          the CUDA-core gate kernel, with its HBM fraction and its relative L2
+          difference from the CUDA-core result.
   --impl reference   the reference's own Dense CPU path (oracle/_ref, compiled
           from the reference sources) on this host, on a bounded prefix of the
           same circuit.
@@ -424,6 +428,33 @@ def run_grover30(tq, device, peak):
     return out
 
 
+def run_block_gate(tq, torch, device, peak, reps=3):
+    import numpy as np
+
+    n, k = 30, 5
+    rng = np.random.default_rng(SEED)
+    q, r = np.linalg.qr(rng.standard_normal((1 << k, 1 << k)) + 1j * rng.standard_normal((1 << k, 1 << k)))
+    u = q * (np.diag(r) / np.abs(np.diag(r)))
+    qubits = np.array([0, 5, 11, 16, 22], dtype=np.uint32)  # index bits 29, 24, 18, 13, 7
+    op = tq.gate(u, qubits)
+    sweep = 2 * 8 * (1 << n)
+    out = {"n_qubits": n, "k": k, "targets": qubits.tolist(), "bytes_per_gate": sweep}
+    states = {}
+    for name, tensor in (("tensor_cores_3xtf32", 1), ("cuda_cores", 0)):
+        g = tq.GpuState(tq.FP32, device)
+        g.set_option(tq.OPT_TENSOR, tensor)
+        g.init_basis(n, 0)
+        g.apply_ops([tq.h(qq) for qq in range(n)])
+        g.apply_ops([op])  # warm-up
+        ms = min(_timed_ops(torch, g, [op]) for _ in range(reps))
+        out[name] = {"ms": ms, "gbs": sweep / (ms / 1e3) / 1e9, "frac": sweep / (ms / 1e3) / 1e9 / peak}
+        states[name] = g
+    out["rel_l2_tensor_vs_cuda_cores"] = states["cuda_cores"].compare(states["tensor_cores_3xtf32"])["rel_l2"]
+    for g in states.values():
+        g.close()
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -529,7 +560,8 @@ def run_ours(args):
         adjoint = run_adjoint(tq, torch, local)
     configs = None
     if rank == 0 and not args.no_configs:
-        configs = {"qft32": run_qft32(tq, torch, local, peak), "grover30": run_grover30(tq, local, peak)}
+        configs = {"qft32": run_qft32(tq, torch, local, peak), "grover30": run_grover30(tq, local, peak),
+                   "block_gate": run_block_gate(tq, torch, local, peak)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

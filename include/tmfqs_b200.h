@@ -120,9 +120,11 @@ typedef enum {
 	                                0: each chain as one twiddle per amplitude from FP64 tables
 	                                (about 1e-15 relative error per pass).  FP32 handles always
 	                                use twiddles. */
-	TMFQS_OPT_RADIX = 5          /* fast forms (FP32 handles, or EXACT=0): 1 (default) passes made only
+	TMFQS_OPT_RADIX = 5,         /* fast forms (FP32 handles, or EXACT=0): 1 (default) passes made only
 	                                of Hadamards and controlled phases run as radix-2^k register
 	                                stages; 0: the general fused pass */
+	TMFQS_OPT_TENSOR = 6         /* FP32 handles: 1 (default) dense 4- and 5-qubit gates run as
+	                                3xTF32 GEMMs on the tensor cores; 0: the CUDA-core gate kernel */
 } tmfqs_option;
 
 /* Kernel classes for tmfqs_gpu_kernel_times. */

@@ -1,0 +1,61 @@
+"""Dense 4- and 5-qubit gates on complex64 states through the tensor cores.
+
+tcgen05 3xTF32 GEMMs (tc_gate.cu) against the FP64 oracle's applyGate
+(gate_block_apply.h:64-213 semantics: targets in block order, first = most
+significant block bit) and against the CUDA-core complex64 gate kernel.
+Tolerance: relative L2 1e-5 (the complex64 form's bound), on two calls in a
+row and for target sets that include the lowest bits (uncoalesced groups).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import tmfqsfullstate_b200 as tq
+
+pytestmark = pytest.mark.gpu
+
+
+def unitary(d, seed):
+    rng = np.random.default_rng(seed)
+    q, r = np.linalg.qr(rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d)))
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+@pytest.mark.parametrize("k", [4, 5])
+@pytest.mark.parametrize("targets", ["high", "low", "mixed"])
+def test_tensor_gate_matches_oracle(k, targets):
+    n = 14
+    rng = np.random.default_rng(k * 10 + len(targets))
+    qubits = {"high": list(range(k)), "low": list(range(n - 1, n - 1 - k, -1)),
+              "mixed": [int(v) for v in rng.permutation(n)[:k]]}[targets]
+    u1, u2 = unitary(1 << k, 1), unitary(1 << k, 2)
+    a = rng.standard_normal(2 << n)
+    a /= np.linalg.norm(a)
+    r = O.OracleRegister(n, amps=a)
+    r.run([O.gate(u1, qubits), O.gate(u2, qubits[::-1])])
+    want = r.amplitudes()
+    outs = []
+    for tensor in (1, 0):
+        with tq.GpuState(tq.FP32) as g:
+            g.set_option(tq.OPT_TENSOR, tensor)
+            g.load(n, a)
+            g.apply_ops([tq.gate(u1, np.array(qubits, dtype=np.uint32))])
+            g.apply_ops([tq.gate(u2, np.array(qubits[::-1], dtype=np.uint32))])
+            outs.append(g.export())
+    assert O.rel_l2(want, outs[0]) < 1e-5
+    assert O.rel_l2(outs[1], outs[0]) < 1e-5
+
+
+def test_tensor_gate_large_state():
+    n, k = 24, 5
+    qubits = [3, 9, 12, 17, 20]
+    u = unitary(1 << k, 7)
+    a = tq.random_phase(n, 5)
+    with tq.GpuState(tq.FP32) as g, tq.GpuState(tq.FP32) as h:
+        g.load(n, a)
+        h.load(n, a)
+        h.set_option(tq.OPT_TENSOR, 0)
+        op = tq.gate(u, np.array(qubits, dtype=np.uint32))
+        g.apply_ops([op])
+        h.apply_ops([op])
+        assert g.compare(h)["rel_l2"] < 1e-6

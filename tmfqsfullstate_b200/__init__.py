@@ -104,6 +104,7 @@ KT_NAMES = ("fused", "permute", "gate", "reduce", "grover", "adjoint")
 OPT_KERNEL_TIMING = 3
 OPT_EXACT = 4
 OPT_RADIX = 5
+OPT_TENSOR = 6
 
 
 class StateComparison(ctypes.Structure):

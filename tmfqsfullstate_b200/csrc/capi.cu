@@ -531,6 +531,16 @@ void validate_op(tmfqs_gpu_state *h, const tmfqs_op &op) {
 }
 
 void run_gate(tmfqs_gpu_state *h, const double *matrix, const unsigned *qubits, unsigned k) {
+	if(h->opt_tensor && tqb::tc_gate_supported(h->precision, h->n, k)) {
+		std::vector<unsigned> tpos(k);
+		for(unsigned i = 0; i < k; ++i) tpos[i] = bit_of(h, qubits[i]);
+		{
+			PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+			tqb::launch_tc_gate(ctx(h), h->amps, h->n, k, matrix, tpos.data(), h->dev_tc, h->dev_tc_bytes);
+		}
+		++h->stats.gate_passes;
+		return;
+	}
 	const size_t dim = 1ull << k;
 	const size_t mbytes = dim * dim * 16;
 	ensure_dev_small(h, mbytes);
@@ -1049,6 +1059,7 @@ int tmfqs_gpu_destroy(tmfqs_gpu_state *h) {
 		}
 		tqb::seq_scratch_free(h->seq);
 		free_adjoint_buffers(h);
+		if(h->dev_tc) cudaFree(h->dev_tc);
 		if(h->amps) cudaFree(h->amps);
 		if(h->dev_small) cudaFree(h->dev_small);
 		if(h->dev_prog) cudaFree(h->dev_prog);
@@ -1072,6 +1083,7 @@ int tmfqs_gpu_clone(tmfqs_gpu_state *h, tmfqs_gpu_state **out) {
 			c->opt_grover_fusion = h->opt_grover_fusion;
 			c->opt_exact = h->opt_exact;
 			c->opt_radix = h->opt_radix;
+			c->opt_tensor = h->opt_tensor;
 			if(h->initialized) {
 				flush_dirty(h);
 				ensure_state(c, h->n);
@@ -1555,6 +1567,7 @@ int tmfqs_gpu_set_option(tmfqs_gpu_state *h, int option, long value) {
 			case TMFQS_OPT_KERNEL_TIMING: h->opt_timing = value != 0; break;
 			case TMFQS_OPT_EXACT: h->opt_exact = value != 0; break;
 			case TMFQS_OPT_RADIX: h->opt_radix = value != 0; break;
+			case TMFQS_OPT_TENSOR: h->opt_tensor = value != 0; break;
 			default: fail(TMFQS_ERR_INVALID_ARGUMENT, "unknown option");
 		}
 	});

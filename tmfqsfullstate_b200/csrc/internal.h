@@ -174,6 +174,16 @@ unsigned launch_grad_run(const LaunchCtx &c, int prec, void *lam, void *psi, uns
                          unsigned count, bool uncompute_psi, double *dev_partials);
 
 // ---------------------------------------------------------------------------
+// Tensor-core dense gates on complex64 states (tc_gate.cu)
+// ---------------------------------------------------------------------------
+bool tc_gate_supported(int prec, unsigned n, unsigned k);
+// matrix_host: row-major 2^k x 2^k interleaved complex (double); tpos: the k
+// target bit positions in block order.  dev_buf is the launcher's reusable
+// device buffer.  Synchronises.
+void launch_tc_gate(const LaunchCtx &c, void *a, unsigned n, unsigned k, const double *matrix_host, const unsigned *tpos,
+                    void *&dev_buf, size_t &dev_buf_bytes);
+
+// ---------------------------------------------------------------------------
 // Device compareStates (compare.cu): the order-independent fields.
 // ---------------------------------------------------------------------------
 struct CompareReport {
@@ -239,6 +249,9 @@ struct tmfqs_gpu_state {
 	bool opt_grover_fusion = true;
 	bool opt_exact = true;
 	bool opt_radix = true;  // fast forms: radix passes where the program allows
+	bool opt_tensor = true; // complex64: 4- and 5-qubit gates on the tensor cores
+	void *dev_tc = nullptr; // tensor-core gate operands
+	size_t dev_tc_bytes = 0;
 	// Adjoint-gradient work buffers, kept for the next call (freed by destroy):
 	// psi checkpoints, FP64 partial sums, and the lambda / psi work states.
 	void *adj_ckpt = nullptr;
