@@ -59,3 +59,49 @@ def test_tensor_gate_large_state():
         g.apply_ops([op])
         h.apply_ops([op])
         assert g.compare(h)["rel_l2"] < 1e-6
+
+
+def brickwork(n, window, layers, seed):
+    """Dense 2-qubit unitaries on neighbouring pairs of `window`, with H / X /
+    CNOT / controlled phases / swaps between them (both libraries' ops)."""
+    rng = np.random.default_rng(seed)
+    ours, theirs = [], []
+    for layer in range(layers):
+        for a in range(layer % 2, len(window) - 1, 2):
+            q = [window[a], window[a + 1]]
+            u = unitary(4, int(rng.integers(1 << 30)))
+            ours.append(tq.gate(u, np.array(q, dtype=np.uint32)))
+            theirs.append(O.gate(u, q))
+            kind = int(rng.integers(0, 5))
+            c, t = (q[0], q[1]) if rng.random() < 0.5 else (q[1], q[0])
+            th = float(rng.uniform(-3, 3))
+            ours.append([tq.h(c), tq.x(t), tq.cnot(c, t), tq.cphase(c, t, th), tq.swap(c, t)][kind])
+            theirs.append([O.h(c), O.x(t), O.cnot(c, t), O.cphase(c, t, th), O.swap(c, t)][kind])
+    return ours, theirs
+
+
+@pytest.mark.parametrize("window", [[3, 4, 5, 6, 7], [9, 10, 11, 12, 13, 14, 15], [0, 2, 4]])
+def test_dense_block_fusion(window):
+    n = 16
+    ours, theirs = brickwork(n, window, 6, len(window))
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal(2 << n)
+    a /= np.linalg.norm(a)
+    r = O.OracleRegister(n, amps=a)
+    r.run(theirs)
+    want = r.amplitudes()
+    outs, passes = [], []
+    for tensor in (1, 0):
+        with tq.GpuState(tq.FP32) as g:
+            g.set_option(tq.OPT_TENSOR, tensor)
+            g.load(n, a)
+            g.reset_stats()
+            g.apply_ops(ours)
+            st = g.stats()
+            passes.append(st["gate_passes"] + st["fused_passes"])
+            outs.append(g.export())
+    assert O.rel_l2(want, outs[0]) < 1e-5
+    assert O.rel_l2(outs[1], outs[0]) < 1e-5
+    if len(window) <= 5:
+        assert passes[0] == 1  # the whole circuit is one block
+    assert passes[0] < passes[1]

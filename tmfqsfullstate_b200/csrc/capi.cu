@@ -6,6 +6,7 @@
 // status codes plus a thread-local message.
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <new>
 #include <string>
@@ -779,6 +780,126 @@ void register_inversion(tmfqs_gpu_state *h, tmfqs_register_view *v, bool materia
 
 // ===========================================================================
 // Public entry points
+// ---- dense-block fusion (complex64 handles, tensor cores) ----
+// The qubits an op acts on, in its own order (first = most significant), and
+// its matrix (row-major, complex); false for ops that cannot join a block.
+bool op_as_matrix(const tmfqs_op &op, std::vector<unsigned> &qs, std::vector<std::complex<double>> &g) {
+	typedef std::complex<double> C;
+	switch(op.kind) {
+		case TMFQS_OP_H: {
+			const double inv = 1.0 / std::sqrt(2.0);  // dense_state_backend.cpp:258
+			qs = {op.q0};
+			g = {C(inv), C(inv), C(inv), C(-inv)};
+			return true;
+		}
+		case TMFQS_OP_X:
+			qs = {op.q0};
+			g = {C(0), C(1), C(1), C(0)};
+			return true;
+		case TMFQS_OP_CNOT:
+			qs = {op.q0, op.q1};
+			g.assign(16, C(0));
+			g[0] = g[5] = g[11] = g[14] = C(1);
+			return true;
+		case TMFQS_OP_CPHASE:
+			qs = {op.q0, op.q1};
+			g.assign(16, C(0));
+			g[0] = g[5] = g[10] = C(1);
+			g[15] = C(std::cos(op.theta), std::sin(op.theta));
+			return true;
+		case TMFQS_OP_SWAP:
+			qs = {op.q0, op.q1};
+			g.assign(16, C(0));
+			g[0] = g[6] = g[9] = g[15] = C(1);
+			return true;
+		case TMFQS_OP_GATE: {
+			if(op.k == 0 || op.k > 5) return false;
+			qs.assign(op.qubits, op.qubits + op.k);
+			const size_t dim = size_t(1) << op.k;
+			g.resize(dim * dim);
+			for(size_t e = 0; e < dim * dim; ++e) g[e] = C(op.matrix[2 * e], op.matrix[2 * e + 1]);
+			return true;
+		}
+		default: return false;
+	}
+}
+
+// Starting at ops[i] (a dense gate), the longest run of ops acting within 5
+// qubits, multiplied in FP64 into one block matrix and applied as one
+// tensor-core gate.  Returns the number of ops consumed (0: no block).
+size_t run_dense_block(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t i, size_t count) {
+	typedef std::complex<double> C;
+	std::vector<unsigned> Q;  // block qubits, block order (first = most significant)
+	std::vector<std::pair<std::vector<unsigned>, std::vector<C>>> parts;
+	size_t j = i;
+	for(; j < count; ++j) {
+		std::vector<unsigned> qs;
+		std::vector<C> g;
+		if(!op_as_matrix(ops[j], qs, g)) break;
+		validate_op(h, ops[j]);
+		std::vector<unsigned> U = Q;
+		for(unsigned q : qs)
+			if(std::find(U.begin(), U.end(), q) == U.end()) U.push_back(q);
+		if(U.size() > 5) break;
+		Q = U;
+		parts.push_back({qs, g});
+	}
+	if(parts.size() < 2) return 0;
+	// Pad to 4 qubits with the highest-order unused ones (identity on them).
+	for(unsigned q = 0; Q.size() < 4 && q < h->n; ++q)
+		if(std::find(Q.begin(), Q.end(), q) == Q.end()) Q.push_back(q);
+	const unsigned s = (unsigned)Q.size();
+	if(!tqb::tc_gate_supported(h->precision, h->n, s)) return 0;
+	const size_t d = size_t(1) << s;
+	std::vector<C> M(d * d, C(0));
+	for(size_t r = 0; r < d; ++r) M[r * d + r] = C(1);
+	std::vector<C> T(d * d);
+	for(const auto &pg : parts) {
+		const std::vector<unsigned> &qs = pg.first;
+		const std::vector<C> &g = pg.second;
+		const unsigned t = (unsigned)qs.size();
+		std::vector<unsigned> bitpos(t);  // block-index bit of each op qubit
+		for(unsigned a = 0; a < t; ++a)
+			bitpos[a] = s - 1 - (unsigned)(std::find(Q.begin(), Q.end(), qs[a]) - Q.begin());
+		auto sub = [&](size_t r) {
+			size_t v = 0;
+			for(unsigned a = 0; a < t; ++a) v |= ((r >> bitpos[a]) & 1u) << (t - 1 - a);
+			return v;
+		};
+		auto with = [&](size_t r, size_t v) {
+			for(unsigned a = 0; a < t; ++a) {
+				const size_t b = (v >> (t - 1 - a)) & 1u;
+				r = (r & ~(size_t(1) << bitpos[a])) | (b << bitpos[a]);
+			}
+			return r;
+		};
+		// T = G (x) I . M
+		const size_t td = size_t(1) << t;
+		for(size_t r = 0; r < d; ++r) {
+			const size_t rv = sub(r);
+			for(size_t c = 0; c < d; ++c) {
+				C acc(0);
+				for(size_t v = 0; v < td; ++v) acc += g[rv * td + v] * M[with(r, v) * d + c];
+				T[r * d + c] = acc;
+			}
+		}
+		M.swap(T);
+	}
+	std::vector<double> mat(2 * d * d);
+	for(size_t e = 0; e < d * d; ++e) {
+		mat[2 * e] = M[e].real();
+		mat[2 * e + 1] = M[e].imag();
+	}
+	std::vector<unsigned> tpos(s);
+	for(unsigned a = 0; a < s; ++a) tpos[a] = bit_of(h, Q[a]);
+	{
+		PassTimer timer(h, TMFQS_KT_GATE, sweep_bytes(h));
+		tqb::launch_tc_gate(ctx(h), h->amps, h->n, s, mat.data(), tpos.data(), h->dev_tc, h->dev_tc_bytes);
+	}
+	++h->stats.gate_passes;
+	return j - i;
+}
+
 // tmfqs_gpu_apply_ops: the Simulator's gate runs through the fusion planner.
 void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count) {
 	ensure_initialized(h, "operation batch");
@@ -819,6 +940,15 @@ void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count) {
 			}
 			if(op.kind == TMFQS_OP_GATE) {
 				p.flush();
+				if(h->precision == TMFQS_FP32 && h->opt_tensor) {
+					// A dense gate and the ops after it that stay within 5 qubits:
+					// one block on the tensor cores.
+					const size_t used = run_dense_block(h, ops, i, count);
+					if(used) {
+						i += used;
+						continue;
+					}
+				}
 				run_gate(h, op.matrix, op.qubits, op.k);
 				++i;
 				continue;
