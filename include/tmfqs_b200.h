@@ -107,6 +107,7 @@ typedef struct {
 	uint64_t gate_passes;       /* single-gate passes over the state */
 	uint64_t reduction_passes;  /* passes of the exact reductions */
 	uint64_t h2d_bytes, d2h_bytes;
+	uint64_t qft_passes;        /* fused passes that ran as the dedicated QFT pass */
 } tmfqs_stats;
 
 /* Tunables (tmfqs_gpu_set_option). */
@@ -123,8 +124,12 @@ typedef enum {
 	TMFQS_OPT_RADIX = 5,         /* fast forms (FP32 handles, or EXACT=0): 1 (default) passes made only
 	                                of Hadamards and controlled phases run as radix-2^k register
 	                                stages; 0: the general fused pass */
-	TMFQS_OPT_TENSOR = 6         /* FP32 handles: 1 (default) dense 4- and 5-qubit gates run as
+	TMFQS_OPT_TENSOR = 6,        /* FP32 handles: 1 (default) dense 4- and 5-qubit gates run as
 	                                3xTF32 GEMMs on the tensor cores; 0: the CUDA-core gate kernel */
+	TMFQS_OPT_QFT_PASS = 7       /* fast forms with RADIX on: 1 (default) passes that are a segment of
+	                                the QFT ladder run as the dedicated QFT pass (per-thread twiddle
+	                                tables, swizzled stages, three tiles in flight); 0: the general
+	                                radix pass */
 } tmfqs_option;
 
 /* Kernel classes for tmfqs_gpu_kernel_times. */

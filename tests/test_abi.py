@@ -33,7 +33,8 @@ def test_struct_layouts_match_header():
     # tmfqs_op: int, 2 x unsigned, double, uint64, int, 2 pointers, unsigned.
     assert ctypes.sizeof(tq.Op) == 64
     assert ctypes.sizeof(tq.RegisterView) == 64
-    assert ctypes.sizeof(tq.Stats) == 48
+    # tmfqs_stats: seven uint64 counters.
+    assert ctypes.sizeof(tq.Stats) == 56
 
 
 def test_create_without_gpu_fails_loudly():

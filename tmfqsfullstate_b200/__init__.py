@@ -105,6 +105,7 @@ OPT_KERNEL_TIMING = 3
 OPT_EXACT = 4
 OPT_RADIX = 5
 OPT_TENSOR = 6
+OPT_QFT_PASS = 7
 
 
 class StateComparison(ctypes.Structure):
@@ -122,6 +123,7 @@ class Stats(ctypes.Structure):
         ("reduction_passes", ctypes.c_uint64),
         ("h2d_bytes", ctypes.c_uint64),
         ("d2h_bytes", ctypes.c_uint64),
+        ("qft_passes", ctypes.c_uint64),
     ]
 
 

@@ -394,8 +394,11 @@ struct Planner {
 			}
 			pass.gate_count = (unsigned)pending.size();
 			PassTimer timer(h, TMFQS_KT_FUSED, sweep_bytes(h));
-			const bool done = twiddle && h->opt_radix &&
-			                  tqb::launch_radix_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes);
+			const bool qft = twiddle && h->opt_radix && h->opt_qft_pass &&
+			                 tqb::launch_qft_pass(ctx(h), h->precision, h->amps, pass);
+			if(qft) ++h->stats.qft_passes;
+			const bool done = qft || (twiddle && h->opt_radix &&
+			                          tqb::launch_radix_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes));
 			if(!done) tqb::launch_fused_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes);
 			++h->stats.fused_passes;
 		}
@@ -978,6 +981,7 @@ tmfqs_gpu_state *work_handle(tmfqs_gpu_state *h, tmfqs_gpu_state *&w) {
 	w->opt_fused_qubits = h->opt_fused_qubits;
 	w->opt_exact = h->opt_exact;
 	w->opt_radix = h->opt_radix;
+	w->opt_qft_pass = h->opt_qft_pass;
 	ensure_state(w, h->n);
 	w->initialized = true;
 	return w;
@@ -1214,6 +1218,7 @@ int tmfqs_gpu_clone(tmfqs_gpu_state *h, tmfqs_gpu_state **out) {
 			c->opt_exact = h->opt_exact;
 			c->opt_radix = h->opt_radix;
 			c->opt_tensor = h->opt_tensor;
+			c->opt_qft_pass = h->opt_qft_pass;
 			if(h->initialized) {
 				flush_dirty(h);
 				ensure_state(c, h->n);
@@ -1698,6 +1703,7 @@ int tmfqs_gpu_set_option(tmfqs_gpu_state *h, int option, long value) {
 			case TMFQS_OPT_EXACT: h->opt_exact = value != 0; break;
 			case TMFQS_OPT_RADIX: h->opt_radix = value != 0; break;
 			case TMFQS_OPT_TENSOR: h->opt_tensor = value != 0; break;
+			case TMFQS_OPT_QFT_PASS: h->opt_qft_pass = value != 0; break;
 			default: fail(TMFQS_ERR_INVALID_ARGUMENT, "unknown option");
 		}
 	});

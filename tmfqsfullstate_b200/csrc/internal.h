@@ -148,6 +148,12 @@ void launch_fused_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &p
 bool launch_radix_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, void *&dev_prog,
                        size_t &dev_prog_bytes);
 
+// The dedicated pass for a segment of the QFT ladder (Hadamards on consecutive
+// descending bits, each followed by the phases pi/2^(b-c) with every lower bit
+// c of the register) in the fast forms.  Returns false (nothing launched) when
+// the pass is not such a segment or its layout does not qualify.
+bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass);
+
 // ---------------------------------------------------------------------------
 // Adjoint gradient (adjoint.cu)
 // ---------------------------------------------------------------------------
@@ -250,6 +256,7 @@ struct tmfqs_gpu_state {
 	bool opt_exact = true;
 	bool opt_radix = true;  // fast forms: radix passes where the program allows
 	bool opt_tensor = true; // complex64: 4- and 5-qubit gates on the tensor cores
+	bool opt_qft_pass = true;  // fast forms: QFT ladder segments on the dedicated QFT pass
 	void *dev_tc = nullptr; // tensor-core gate operands
 	size_t dev_tc_bytes = 0;
 	// Adjoint-gradient work buffers, kept for the next call (freed by destroy):

@@ -1,0 +1,568 @@
+// QFT segment passes for the fast forms (complex64 states, and complex128 with
+// TMFQS_OPT_EXACT off).
+//
+// A pass of the QFT ladder (circuit::appendQft, circuit.cpp:87-100) covers a
+// run of qubits whose index bits b are consecutive and descending: H on b,
+// then the controlled phases pi/2^(b-c) with every lower bit c of the
+// register (c >= r0).  In the pass:
+//   - the Hadamards and the phases between the run's own bits form a small
+//     QFT on those bits, done in registers as compiled ladders of up to RB bits
+//     (one "stage" each: the 2^RB amplitudes of a thread differ in the stage's
+//     bits);
+//   - the phases between a stage's bits and every lower bit c (later stages,
+//     the low local bits, outer bits) commute with the rest of the stage, so
+//     they are applied after it as one twiddle per amplitude:
+//         exp(2*pi*i * W / 2^(b+1)) for each stage bit b in state |1>,
+//     W = the value of the bits in [r0, lowest bit of the stage).
+//     The factor of bit b splits into a per-thread part (the local bits of W:
+//     the same for every tile, tabulated per thread at the start of the
+//     launch) and a per-tile part (the outer bits of W, computed by one thread
+//     per stage while the tile's copies are in flight).  Both come from
+//     sincospi in FP64 and FP64 squarings, each rounded once.
+// Tiles of 2^K amplitudes stream through a ring of shared-memory buffers with
+// 16-byte cp.async copies (two tiles in flight behind the one being
+// transformed); a thread's copies sit at fixed offsets from the tile base.  Stage accesses use an XOR swizzle chosen per pass on the
+// host so that the lanes of each half-warp (quarter-warp for complex128) hit
+// distinct banks wherever the pass's bit layout allows it.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "device_common.cuh"
+#include "internal.h"
+#include "radix_common.cuh"
+
+namespace tqb {
+
+namespace {
+
+constexpr unsigned kQftMaxThreads = 256;
+constexpr unsigned kQftMaxStages = 4;
+constexpr unsigned kQftMaxRuns = 8;
+constexpr unsigned kQftGranules = 16;  // 16-byte granules per thread per tile
+constexpr uint32_t kQftNone = 0xffffffffu;
+
+struct QftStage {
+	uint32_t d;           // Hadamards of the stage: register bits 0..d-1, in circuit order
+	uint32_t bhi;         // global bit of register bit 0 (register bit i < d is bit bhi - i)
+	uint32_t rsorted[5];  // the register local bits, ascending
+	uint32_t roff[5];     // swizzled shared-memory offset (elements) of register bit i
+	uint32_t fl;          // first per-thread factor row, kQftNone: no twiddle
+	uint32_t ot;          // first per-tile factor in a factor row, kQftNone: none
+	uint32_t scaled;      // the pass's real scale (1/sqrt(2))^P is applied here
+	uint32_t pad;
+	uint64_t wmask;       // the bits of W: [r0, lowest Hadamard bit of the stage)
+};
+
+struct QftGeom {
+	uint32_t K;        // local bits: tiles of 2^K amplitudes
+	uint32_t nstages;
+	uint32_t slots;    // tile buffers in the ring (2 or 3)
+	uint32_t nruns;    // runs of outer bits, ascending: tile index bits in order
+	uint32_t run_pos[kQftMaxRuns], run_len[kQftMaxRuns];
+	uint32_t lpos[16];               // local bit -> global bit
+	uint32_t sw_src[3], sw_dst[3];   // swizzle: shared index bit sw_dst[k] ^= index bit sw_src[k] (src 0: none)
+	uint32_t ot_stride;  // storage values per per-tile factor row (16-byte rows), 0: none
+	uint32_t nfrows;     // per-thread factor rows
+	uint64_t localmask;
+	uint64_t ntiles;
+	uint64_t istride;    // global element step between a thread's granules
+	double scale;
+	QftStage st[kQftMaxStages];
+	RootTable roots;
+};
+
+template <typename V>
+struct Scalar;
+template <>
+struct Scalar<float2> {
+	typedef float type;
+};
+template <>
+struct Scalar<double2> {
+	typedef double type;
+};
+
+template <typename V>
+__device__ __forceinline__ V vscale(V v, typename Scalar<V>::type s) {
+	v.x *= s;
+	v.y *= s;
+	return v;
+}
+
+template <typename V>
+__device__ __forceinline__ V to_storage(double x, double y) {
+	V z;
+	z.x = (typename Scalar<V>::type)x;
+	z.y = (typename Scalar<V>::type)y;
+	return z;
+}
+
+// dst[i * stride] = exp(2*pi*i * w / 2^(bhi+1-i)), i < d: the twiddles of
+// the stage bits bhi, bhi-1, ... for W = w.  The first from sincospi in FP64
+// (w < 2^bhi, so the argument is exact), the rest by squaring in FP64; each
+// rounded once to the storage type.
+template <typename V>
+__device__ __forceinline__ void stage_factors(uint64_t w, unsigned bhi, unsigned d, V *dst, unsigned stride) {
+	double s, c;
+	sincospi(ldexp((double)w, -(int)bhi), &s, &c);
+	for(unsigned i = 0; i < d; ++i) {
+		dst[i * stride] = to_storage<V>(c, s);
+		const double c2 = c * c - s * s, s2 = 2.0 * c * s;
+		c = c2;
+		s = s2;
+	}
+}
+
+__device__ __forceinline__ unsigned qft_phys(const QftGeom &g, unsigned j) {
+	unsigned x = j;
+#pragma unroll
+	for(int k = 0; k < 3; ++k)
+		if(g.sw_src[k]) x ^= ((j >> g.sw_src[k]) & 1u) << g.sw_dst[k];
+	return x;
+}
+
+__device__ __forceinline__ uint64_t qft_scatter(const QftGeom &g, unsigned j) {
+	uint64_t x = 0;
+	for(unsigned l = 0; l < g.K; ++l)
+		if((j >> l) & 1u) x |= 1ull << g.lpos[l];
+	return x;
+}
+
+// Global element offset of the first amplitude of tile o: the bits of o
+// deposited into the runs of outer bits.
+__device__ __forceinline__ uint64_t qft_tile_base(const QftGeom &g, uint64_t o) {
+	uint64_t base = 0;
+	for(unsigned k = 0; k < g.nruns; ++k) {
+		const unsigned len = g.run_len[k];
+		base |= (o & ((1ull << len) - 1ull)) << g.run_pos[k];
+		o >>= len;
+	}
+	return base;
+}
+
+// v[r] times prod_{i < D, r_i = 1} f[i] (the filler bits D.. carry no factor),
+// and the real scale s on every value when SC.  The products come from two
+// small tables over bits 0..2 and 3..D-1: at most two complex products per
+// amplitude, few registers.
+template <typename V, int RB, int D, bool SC>
+__device__ __forceinline__ void apply_twiddle(V (&v)[1 << RB], const V (&f)[D], typename Scalar<V>::type s) {
+	constexpr int LO = D < 3 ? D : 3, HI = D - LO;
+	V FL[1 << LO], FH[1 << HI];
+#pragma unroll
+	for(int k = 1; k < (1 << LO); ++k) {
+		const int hb = 31 - __clz(k);
+		FL[k] = (k == (1 << hb)) ? f[hb] : vmul(FL[k ^ (1 << hb)], f[hb]);
+	}
+#pragma unroll
+	for(int k = 1; k < (1 << HI); ++k) {
+		const int hb = 31 - __clz(k);
+		FH[k] = (k == (1 << hb)) ? f[LO + hb] : vmul(FH[k ^ (1 << hb)], f[LO + hb]);
+	}
+	if constexpr(SC) {
+#pragma unroll
+		for(int k = 1; k < (1 << LO); ++k) FL[k] = vscale(FL[k], s);
+	}
+#pragma unroll
+	for(int r = 0; r < (1 << RB); ++r) {
+		const int k = r & ((1 << D) - 1), lo = k & ((1 << LO) - 1), hi = k >> LO;
+		if(lo) v[r] = vmul(v[r], FL[lo]);
+		else if(SC) v[r] = vscale(v[r], s);
+		if(hi) v[r] = vmul(v[r], FH[hi]);
+	}
+}
+
+// One stage on the tile in shared memory: the thread's 2^RB amplitudes are
+// read, transformed (ladder, twiddle, scale) and written back in place.
+template <typename V, int RB, int D, bool TW, bool SC>
+__device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
+                                              const V *ot, typename Scalar<V>::type s, const RootTable &roots) {
+	unsigned roff[RB];
+#pragma unroll
+	for(int i = 0; i < RB; ++i) roff[i] = S.roff[i];
+	V v[1 << RB];
+#pragma unroll
+	for(int r = 0; r < (1 << RB); ++r) {
+		unsigned x = pbase;
+#pragma unroll
+		for(int i = 0; i < RB; ++i)
+			if((r >> i) & 1) x ^= roff[i];
+		v[r] = tile[x];
+	}
+	qft_stage<V, RB, D>(v, roots);
+	if constexpr(TW) {
+		V f[D];
+#pragma unroll
+		for(int i = 0; i < D; ++i) f[i] = frow[i * nthr];
+		const unsigned oc = S.ot;
+		if(oc != kQftNone) {
+#pragma unroll
+			for(int i = 0; i < D; ++i) f[i] = vmul(f[i], ot[oc + i]);
+		}
+		apply_twiddle<V, RB, D, SC>(v, f, s);
+	} else if constexpr(SC) {
+#pragma unroll
+		for(int r = 0; r < (1 << RB); ++r) v[r] = vscale(v[r], s);
+	}
+#pragma unroll
+	for(int r = 0; r < (1 << RB); ++r) {
+		unsigned x = pbase;
+#pragma unroll
+		for(int i = 0; i < RB; ++i)
+			if((r >> i) & 1) x ^= roff[i];
+		tile[x] = v[r];
+	}
+}
+
+template <typename V, int RB, int D>
+__device__ __forceinline__ void qft_stage_flags(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
+                                                const V *ot, typename Scalar<V>::type s, const RootTable &roots) {
+	const bool tw = S.fl != kQftNone;
+	if(tw) {
+		if(S.scaled) qft_stage_run<V, RB, D, true, true>(tile, S, pbase, frow, nthr, ot, s, roots);
+		else qft_stage_run<V, RB, D, true, false>(tile, S, pbase, frow, nthr, ot, s, roots);
+	} else {
+		if(S.scaled) qft_stage_run<V, RB, D, false, true>(tile, S, pbase, frow, nthr, ot, s, roots);
+		else qft_stage_run<V, RB, D, false, false>(tile, S, pbase, frow, nthr, ot, s, roots);
+	}
+}
+
+template <typename V, int RB>
+__device__ __forceinline__ void qft_stage_dispatch(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
+                                                   const V *ot, typename Scalar<V>::type s, const RootTable &roots) {
+	switch(S.d) {
+		case 1: qft_stage_flags<V, RB, 1>(tile, S, pbase, frow, nthr, ot, s, roots); break;
+		case 2: qft_stage_flags<V, RB, 2>(tile, S, pbase, frow, nthr, ot, s, roots); break;
+		case 3: qft_stage_flags<V, RB, 3>(tile, S, pbase, frow, nthr, ot, s, roots); break;
+		case 4: qft_stage_flags<V, RB, 4>(tile, S, pbase, frow, nthr, ot, s, roots); break;
+		case 5: if constexpr(RB >= 5) qft_stage_flags<V, RB, 5>(tile, S, pbase, frow, nthr, ot, s, roots); break;
+		default: break;
+	}
+}
+
+// The pass.  Shared memory: the ring of tile buffers, the stage descriptors,
+// the per-thread twiddle factors [nfrows][nthr], the swizzled index of each
+// thread's first amplitude per stage [nstages][nthr], and one row of per-tile
+// factors per ring slot.  Everything is derived here from the geometry: the
+// launch needs no device program.
+template <typename R, int RB>
+__global__ void __launch_bounds__(kQftMaxThreads, 1)
+	k_qft_pass(typename Vec2<R>::type *a, const __grid_constant__ QftGeom g) {
+	typedef typename Vec2<R>::type V;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	constexpr unsigned per16 = 16 / sizeof(V);
+	const unsigned T = 1u << g.K, tid = threadIdx.x, nthr = blockDim.x;
+	V *ring = reinterpret_cast<V *>(smem_raw);
+	V *ftab = ring + (size_t)g.slots * T;
+	V *orow = ftab + (size_t)g.nfrows * nthr;
+	QftStage *sst = reinterpret_cast<QftStage *>(orow + (size_t)g.slots * g.ot_stride);
+	uint32_t *spst = reinterpret_cast<uint32_t *>(sst + kQftMaxStages);
+
+	if(tid < g.nstages) sst[tid] = g.st[tid];
+	const uint64_t goff = qft_scatter(g, tid * per16);
+	const unsigned psm = qft_phys(g, tid * per16);
+	const unsigned gstep = nthr * per16;  // shared index step between a thread's granules
+	__syncthreads();
+
+	// Tile o's amplitudes (16-byte granules at fixed per-thread offsets) and,
+	// from one thread per stage, its row of per-tile factors (the outer bits
+	// of W), computed while the copies are in flight.
+	auto prefetch = [&](uint64_t o, unsigned slot) {
+		if(o < g.ntiles) {
+			const uint64_t base = qft_tile_base(g, o);
+			const V *src = a + base + goff;
+			V *dst = ring + (size_t)slot * T + psm;
+#pragma unroll
+			for(unsigned i = 0; i < kQftGranules; ++i) cp_async16(dst + i * gstep, src + i * g.istride);
+			cp_async_commit();
+			const unsigned st = tid >> 5;
+			if((tid & 31u) == 0 && st < g.nstages && sst[st].ot != kQftNone)
+				stage_factors<V>(base & sst[st].wmask & ~g.localmask, sst[st].bhi, sst[st].d,
+				                 orow + slot * g.ot_stride + sst[st].ot, 1);
+		} else {
+			cp_async_commit();
+		}
+	};
+	uint64_t o = blockIdx.x;
+	for(unsigned k = 0; k + 1 < g.slots; ++k) prefetch(o + (uint64_t)k * gridDim.x, k);
+
+	// Per-thread tables (once per launch).
+	for(unsigned st = 0; st < g.nstages; ++st) {
+		const QftStage &S = sst[st];
+		unsigned jt = tid;
+		for(unsigned i = 0; i < RB; ++i) {
+			const unsigned b = S.rsorted[i], lo = jt & ((1u << b) - 1u);
+			jt = ((jt ^ lo) << 1) | lo;
+		}
+		spst[st * nthr + tid] = qft_phys(g, jt);
+		if(S.fl != kQftNone) stage_factors<V>(qft_scatter(g, jt) & S.wmask, S.bhi, S.d, ftab + (size_t)S.fl * nthr + tid, nthr);
+	}
+
+	const typename Scalar<V>::type s = (typename Scalar<V>::type)g.scale;
+	unsigned slot = 0;
+	for(; o < g.ntiles; o += gridDim.x) {
+		if(g.slots == 3) cp_async_wait1();
+		else cp_async_wait_all();
+		__syncthreads();
+		prefetch(o + (uint64_t)(g.slots - 1) * gridDim.x, slot == 0 ? g.slots - 1 : slot - 1);
+		V *tile = ring + (size_t)slot * T;
+		const V *ot = orow + slot * g.ot_stride;
+		for(unsigned st = 0; st < g.nstages; ++st) {
+			const QftStage &S = sst[st];
+			const V *frow = ftab + (size_t)(S.fl == kQftNone ? 0u : S.fl) * nthr + tid;
+			qft_stage_dispatch<V, RB>(tile, S, spst[st * nthr + tid], frow, nthr, ot, s, g.roots);
+			__syncthreads();
+		}
+		V *dst = a + qft_tile_base(g, o) + goff;
+		const V *src = tile + psm;
+#pragma unroll
+		for(unsigned i = 0; i < kQftGranules; ++i)
+			*reinterpret_cast<float4 *>(dst + i * g.istride) = *reinterpret_cast<const float4 *>(src + i * gstep);
+		slot = slot + 1 == g.slots ? 0 : slot + 1;
+	}
+	cp_async_wait_all();
+}
+
+// ---------------------------------------------------------------------------
+// Host side: recognising a QFT segment and planning its pass.
+
+// Hadamards on consecutive descending bits hb[0] > hb[1] > ..., each followed
+// by the controlled phases pi/2^(b-c) with every bit c in [r0, b) (in any
+// order), and nothing else.  r0 = n when the segment has no phases.
+bool qft_segment(const FusedPass &pass, std::vector<unsigned> &hb, unsigned &r0) {
+	hb.clear();
+	r0 = pass.n;
+	bool have_r0 = false, bare = false;
+	const double pi = std::acos(-1.0);
+	for(const FusedOp &f : pass.ops) {
+		if(f.kind != kFH && f.kind != kFHChain && f.kind != kFHTwiddle) return false;
+		if(f.lt >= pass.K) return false;
+		const unsigned b = pass.lpos[f.lt];
+		if(!hb.empty() && b + 1 != hb.back()) return false;
+		const unsigned cnt = f.kind == kFH ? 0u : f.lc;
+		uint64_t seen = 0;
+		unsigned lo = b;
+		for(unsigned e = 0; e < cnt; ++e) {
+			const ChainEntry &ce = pass.chain[f.tab + e];
+			const unsigned c = ce.bit;
+			if(c >= b || ((seen >> c) & 1ull)) return false;
+			seen |= 1ull << c;
+			lo = std::min(lo, c);
+			const double want = std::ldexp(pi, -(int)(b - c));
+			if(!(std::fabs(ce.theta - want) <= 1e-12 * want)) return false;
+		}
+		if(cnt != b - lo) return false;  // the phases cover [lo, b) exactly
+		if(cnt) {
+			if(bare) return false;  // an earlier, higher Hadamard lacked its phases
+			if(!have_r0) {
+				r0 = lo;
+				have_r0 = true;
+			} else if(lo != r0) {
+				return false;
+			}
+		} else {
+			if(have_r0 && b > r0) return false;
+			if(!have_r0) bare = true;
+		}
+		hb.push_back(b);
+	}
+	return !hb.empty();
+}
+
+inline unsigned insert_zeros(unsigned t, const uint32_t *sorted, int count) {
+	for(int i = 0; i < count; ++i) {
+		const unsigned b = sorted[i], lo = t & ((1u << b) - 1u);
+		t = ((t ^ lo) << 1) | lo;
+	}
+	return t;
+}
+
+struct Swizzle {
+	unsigned src[3] = {0, 0, 0}, dst[3] = {0, 0, 0};
+	unsigned operator()(unsigned j) const {
+		unsigned x = j;
+		for(int k = 0; k < 3; ++k)
+			if(src[k]) x ^= ((j >> src[k]) & 1u) << dst[k];
+		return x;
+	}
+};
+
+// Plans the pass for storage values of vbytes bytes and RB register bits.
+bool plan_qft(const FusedPass &pass, unsigned vbytes, unsigned RB, QftGeom &g) {
+	std::vector<unsigned> hb;
+	unsigned r0 = 0;
+	if(!qft_segment(pass, hb, r0)) return false;
+	const unsigned K = pass.K, n = pass.n, per16 = 16 / vbytes;
+	if(K < RB + 5 || K - RB > 8 || K < 4) return false;
+	if(pass.lpos[K - 1] - pass.lpos[K - 4] != 3) return false;  // the granule index bits are contiguous
+	if(per16 == 2 && pass.lpos[0] != 0) return false;            // two adjacent amplitudes per granule
+	auto li = [&](unsigned bit) -> int {
+		for(unsigned i = 0; i < K; ++i)
+			if(pass.lpos[i] == bit) return (int)i;
+		return -1;
+	};
+	const unsigned np = (unsigned)hb.size(), nst = (np + RB - 1) / RB;
+	if(nst > kQftMaxStages) return false;
+	g = QftGeom{};
+	g.K = K;
+	g.nstages = nst;
+	g.ntiles = 1ull << (n - K);
+	g.istride = 1ull << pass.lpos[K - 4];
+	for(unsigned i = 0; i < K; ++i) {
+		g.lpos[i] = pass.lpos[i];
+		g.localmask |= 1ull << pass.lpos[i];
+	}
+	fill_roots(g.roots);
+	auto range_mask = [](unsigned lo, unsigned hi) -> uint64_t {
+		if(hi <= lo) return 0ull;
+		const uint64_t top = hi >= 64 ? ~0ull : ((1ull << hi) - 1ull);
+		return top & ~((1ull << lo) - 1ull);
+	};
+
+	// Stages: register bits 0..d-1 are the stage's Hadamard bits in circuit
+	// order; the rest are filler bits outside the twiddle range (above the
+	// stage, or below r0).
+	uint32_t rbit[kQftMaxStages][5] = {};
+	unsigned nfrows = 0, ocol = 0;
+	for(unsigned s = 0; s < nst; ++s) {
+		QftStage &S = g.st[s];
+		const unsigned first = s * RB;
+		S.d = std::min(RB, np - first);
+		const unsigned hi = hb[first], lo = hb[first + S.d - 1];
+		S.bhi = hi;
+		S.wmask = range_mask(r0, lo);
+		uint32_t used = 0;
+		for(unsigned i = 0; i < S.d; ++i) {
+			const int l = li(hb[first + i]);
+			if(l < 0) return false;
+			rbit[s][i] = (uint32_t)l;
+			used |= 1u << l;
+		}
+		unsigned cnt = S.d;
+		for(int l = (int)K - 1; l >= 0 && cnt < RB; --l)
+			if(!((used >> l) & 1u) && pass.lpos[l] > hi) {
+				rbit[s][cnt++] = (uint32_t)l;
+				used |= 1u << l;
+			}
+		for(unsigned l = 0; l < K && cnt < RB; ++l)
+			if(!((used >> l) & 1u) && pass.lpos[l] < r0) {
+				rbit[s][cnt++] = l;
+				used |= 1u << l;
+			}
+		if(cnt < RB) return false;
+		std::vector<uint32_t> srt(rbit[s], rbit[s] + RB);
+		std::sort(srt.begin(), srt.end());
+		for(unsigned i = 0; i < RB; ++i) S.rsorted[i] = srt[i];
+		S.fl = kQftNone;
+		S.ot = kQftNone;
+		if(S.wmask) {
+			S.fl = nfrows;
+			nfrows += S.d;
+			if(S.wmask & ~g.localmask) {
+				S.ot = ocol;
+				ocol += S.d;
+			}
+		}
+		S.scaled = s + 1 == nst;
+	}
+	g.nfrows = nfrows;
+	g.ot_stride = ocol;
+
+	// Swizzle: shared index bits dst ^= local bits src, the sources among the
+	// thread bits of the copies (so a thread's granules stay at fixed offsets),
+	// chosen so that each stage's half-warps (quarter-warps for 16-byte
+	// amplitudes) hit as few banks twice as the layout allows.
+	const unsigned bank_mask = per16 == 2 ? 15u : 7u, group = per16 == 2 ? 16u : 8u;
+	const unsigned dst0 = per16 == 2 ? 1u : 0u, src_lo = per16 == 2 ? 4u : 3u, src_hi = K - 5;
+	auto cost = [&](const Swizzle &w) {
+		unsigned total = 0;
+		for(unsigned s = 0; s < nst; ++s) {
+			unsigned count[16] = {0}, worst = 0;
+			for(unsigned lane = 0; lane < group; ++lane) {
+				const unsigned b = w(insert_zeros(lane, g.st[s].rsorted, (int)RB)) & bank_mask;
+				worst = std::max(worst, ++count[b]);
+			}
+			total += worst;
+		}
+		return total;
+	};
+	std::vector<unsigned> cand{0};
+	for(unsigned b = src_lo; b <= src_hi; ++b) cand.push_back(b);
+	Swizzle best;
+	for(int k = 0; k < 3; ++k) best.dst[k] = dst0 + k;
+	unsigned best_cost = cost(best), best_used = 0;
+	for(unsigned x : cand)
+		for(unsigned y : cand)
+			for(unsigned z : cand) {
+				Swizzle w = best;
+				w.src[0] = x;
+				w.src[1] = y;
+				w.src[2] = z;
+				const unsigned used = (x != 0) + (y != 0) + (z != 0);
+				const unsigned cc = cost(w);
+				if(cc < best_cost || (cc == best_cost && used < best_used)) {
+					best = w;
+					best_cost = cc;
+					best_used = used;
+				}
+			}
+	for(int k = 0; k < 3; ++k) {
+		g.sw_src[k] = best.src[k];
+		g.sw_dst[k] = best.dst[k];
+	}
+	for(unsigned s = 0; s < nst; ++s)
+		for(unsigned i = 0; i < RB; ++i) g.st[s].roff[i] = best(1u << rbit[s][i]);
+
+	// Runs of outer bits, ascending.
+	g.nruns = 0;
+	for(unsigned b = 0; b < n;) {
+		if((g.localmask >> b) & 1ull) {
+			++b;
+			continue;
+		}
+		unsigned e = b;
+		while(e < n && !((g.localmask >> e) & 1ull)) ++e;
+		if(g.nruns == kQftMaxRuns) return false;
+		g.run_pos[g.nruns] = b;
+		g.run_len[g.nruns] = e - b;
+		++g.nruns;
+		b = e;
+	}
+	g.scale = std::ldexp((np & 1u) ? 1.0 / std::sqrt(2.0) : 1.0, -(int)(np / 2));
+	return true;
+}
+
+template <typename R, int RB>
+bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass) {
+	typedef typename Vec2<R>::type V;
+	QftGeom g;
+	if(!plan_qft(pass, (unsigned)sizeof(V), (unsigned)RB, g)) return false;
+	const unsigned nthr = 1u << (g.K - RB);
+	const size_t T = size_t(1) << g.K;
+	auto smem_for = [&](unsigned slots) {
+		return (slots * T + (size_t)g.nfrows * nthr + (size_t)slots * g.ot_stride) * sizeof(V) +
+		       kQftMaxStages * sizeof(QftStage) + (size_t)g.nstages * nthr * 4;
+	};
+	int dev = 0, max_optin = 0;
+	check_cuda(cudaGetDevice(&dev), "qft device");
+	check_cuda(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "qft smem limit");
+	g.slots = smem_for(3) <= (size_t)max_optin ? 3u : 2u;
+	const size_t smem = smem_for(g.slots);
+	if(smem > (size_t)max_optin) return false;
+	check_cuda(cudaFuncSetAttribute(k_qft_pass<R, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "qft smem");
+	const uint64_t grid = std::min<uint64_t>(g.ntiles, (uint64_t)c.num_sms);
+	k_qft_pass<R, RB><<<(unsigned)grid, nthr, smem, c.stream>>>(static_cast<V *>(a), g);
+	check_cuda(cudaGetLastError(), "qft pass");
+	if(c.launches) ++*c.launches;
+	return true;
+}
+
+}  // namespace
+
+bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass) {
+	if(prec == TMFQS_FP64) return run_qft<double, 4>(c, a, pass);
+	return run_qft<float, 5>(c, a, pass);
+}
+
+}  // namespace tqb

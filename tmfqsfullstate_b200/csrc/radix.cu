@@ -30,6 +30,7 @@
 
 #include "device_common.cuh"
 #include "internal.h"
+#include "radix_common.cuh"
 
 namespace tqb {
 
@@ -52,10 +53,6 @@ constexpr unsigned kRadixMaxSlots = 48;
 //                   controlled phases pi/2^(j-i) with every later bit j, as a
 //                   compiled butterfly network with the roots of unity below
 enum RadixItemKind : uint32_t { kRIButterfly = 0, kRIButterflyTw = 1, kRIDiag = 2, kRIQft = 3 };
-
-// cos and sin of 2*pi*k/32, k < 16 (host C library, FP64): the twiddles of
-// the compiled QFT stages.
-constexpr unsigned kRoots = 16;
 
 struct RadixStage {
 	uint32_t first, count;    // items of the stage
@@ -93,13 +90,8 @@ struct RadixGeom {
 	unsigned lpos[14];          // ascending local bit positions
 	uint64_t ntiles;
 	unsigned nstages, nitems, ntab, nslots, nterms;
-	double root[kRoots][2];     // FP64 roots (complex128 states)
-	float rootf[kRoots][2];     // the same rounded once (complex64 states)
+	RootTable roots;            // twiddles of the compiled QFT stages
 };
-
-// Root k as a storage-type value, read from the kernel parameters.
-__device__ __forceinline__ void root_of(const RadixGeom &g, int k, double2 &r) { r = make_double2(g.root[k][0], g.root[k][1]); }
-__device__ __forceinline__ void root_of(const RadixGeom &g, int k, float2 &r) { r = make_float2(g.rootf[k][0], g.rootf[k][1]); }
 
 template <typename V>
 struct RadixSmem {
@@ -125,21 +117,7 @@ __device__ __forceinline__ unsigned rswz<float2>(unsigned j) {
 	return j ^ (((j >> 4) & 7u) << 1);
 }
 
-template <typename R>
-__device__ __forceinline__ void cmul_fma(R pr, R pi, R &re, R &im) {
-	const R nr = fma(pr, re, -(pi * im));
-	const R ni = fma(pr, im, pi * re);
-	re = nr;
-	im = ni;
-}
 
-template <typename V>
-__device__ __forceinline__ V vmul(V a, V b) {
-	V r;
-	r.x = fma(a.x, b.x, -(a.y * b.y));
-	r.y = fma(a.x, b.y, a.y * b.x);
-	return r;
-}
 
 
 __device__ __forceinline__ unsigned rinsert0(unsigned x, unsigned b) {
@@ -167,19 +145,6 @@ __device__ __forceinline__ double2 to_v<double2>(double2 d) {
 template <>
 __device__ __forceinline__ float2 to_v<float2>(double2 d) {
 	return make_float2((float)d.x, (float)d.y);
-}
-
-// One unscaled butterfly: (x, y) <- (x + y, x - y).  Complex64 values use
-// the paired FP32 instructions (one instruction per complex add).
-__device__ __forceinline__ void bfly2(double2 &x, double2 &y) {
-	const double2 a = x, b = y;
-	x = make_double2(a.x + b.x, a.y + b.y);
-	y = make_double2(a.x - b.x, a.y - b.y);
-}
-__device__ __forceinline__ void bfly2(float2 &x, float2 &y) {
-	const float2 a = x, b = y;
-	x = __fadd2_rn(a, b);
-	y = __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
 }
 
 // Butterflies on register bit TB (unscaled); with `tw`, the |1> output of
@@ -213,77 +178,14 @@ __device__ __forceinline__ void rbfly_dispatch(V (&v)[1 << RB], unsigned b, cons
 	}
 }
 
-// v times exp(2*pi*i*k/32), k < 16 known at compile time: exact for k = 0 and
-// k = 8 (the factor i), otherwise a complex product with the tabulated root.
-template <int k, typename V>
-__device__ __forceinline__ V mul_root(V v, const RadixGeom &g) {
-	if constexpr(k == 0) {
-		return v;
-	} else if constexpr(k == 8) {
-		V r;
-		r.x = -v.y;
-		r.y = v.x;
-		return r;
-	} else {
-		V w;
-		root_of(g, k, w);
-		return vmul(v, w);
-	}
-}
-
-// The QFT ladder on register bits 0..D-1.  After the butterflies on bit i,
-// the |1> output at register r gets exp(2*pi*i*K/2^(D-i)) with
-// K = sum_{j>i} r_j 2^(D-1-j): the phases pi/2^(j-i) of the controlled phases
-// between bit i and each later bit j.
-template <typename V, int RB, int D>
-__device__ __forceinline__ void qft_stage(V (&v)[1 << RB], const RadixGeom &g) {
-#pragma unroll
-	for(int i = 0; i < D; ++i) {
-#pragma unroll
-		for(int q = 0; q < (1 << (RB - 1)); ++q) {
-			const int lo = (1 << i) - 1;
-			const int r0 = ((q & ~lo) << 1) | (q & lo), r1 = r0 | (1 << i);
-			bfly2(v[r0], v[r1]);
-		}
-#pragma unroll
-		for(int r = 0; r < (1 << RB); ++r) {
-			if(!((r >> i) & 1)) continue;
-			int K = 0;
-#pragma unroll
-			for(int j = i + 1; j < D; ++j) K |= ((r >> j) & 1) << (D - 1 - j);
-			// exp(2 pi i K / 2^(D-i)) = root[K * 32 / 2^(D-i)]
-			const int idx = K << (5 - (D - i));
-			switch(idx) {
-				case 0: break;
-				case 1: v[r] = mul_root<1>(v[r], g); break;
-				case 2: v[r] = mul_root<2>(v[r], g); break;
-				case 3: v[r] = mul_root<3>(v[r], g); break;
-				case 4: v[r] = mul_root<4>(v[r], g); break;
-				case 5: v[r] = mul_root<5>(v[r], g); break;
-				case 6: v[r] = mul_root<6>(v[r], g); break;
-				case 7: v[r] = mul_root<7>(v[r], g); break;
-				case 8: v[r] = mul_root<8>(v[r], g); break;
-				case 9: v[r] = mul_root<9>(v[r], g); break;
-				case 10: v[r] = mul_root<10>(v[r], g); break;
-				case 11: v[r] = mul_root<11>(v[r], g); break;
-				case 12: v[r] = mul_root<12>(v[r], g); break;
-				case 13: v[r] = mul_root<13>(v[r], g); break;
-				case 14: v[r] = mul_root<14>(v[r], g); break;
-				case 15: v[r] = mul_root<15>(v[r], g); break;
-				default: break;
-			}
-		}
-	}
-}
-
 template <typename V, int RB>
 __device__ __forceinline__ void qft_dispatch(V (&v)[1 << RB], unsigned d, const RadixGeom &g) {
 	switch(d) {
-		case 1: qft_stage<V, RB, 1>(v, g); break;
-		case 2: if constexpr(RB >= 2) qft_stage<V, RB, 2>(v, g); break;
-		case 3: if constexpr(RB >= 3) qft_stage<V, RB, 3>(v, g); break;
-		case 4: if constexpr(RB >= 4) qft_stage<V, RB, 4>(v, g); break;
-		case 5: if constexpr(RB >= 5) qft_stage<V, RB, 5>(v, g); break;
+		case 1: qft_stage<V, RB, 1>(v, g.roots); break;
+		case 2: if constexpr(RB >= 2) qft_stage<V, RB, 2>(v, g.roots); break;
+		case 3: if constexpr(RB >= 3) qft_stage<V, RB, 3>(v, g.roots); break;
+		case 4: if constexpr(RB >= 4) qft_stage<V, RB, 4>(v, g.roots); break;
+		case 5: if constexpr(RB >= 5) qft_stage<V, RB, 5>(v, g.roots); break;
 		default: break;
 	}
 }
@@ -585,13 +487,7 @@ bool build_radix_program(const FusedPass &pass, unsigned K, size_t vbytes, Radix
 	while(g.m < K && pass.lpos[g.m] == g.m) ++g.m;
 	g.ntiles = 1ull << (pass.n - K);
 	g.lo = (K + 1) / 2;
-	const double two_pi = 2.0 * std::acos(-1.0);
-	for(unsigned k = 0; k < kRoots; ++k) {
-		g.root[k][0] = std::cos(two_pi * k / 32.0);
-		g.root[k][1] = std::sin(two_pi * k / 32.0);
-		g.rootf[k][0] = (float)g.root[k][0];
-		g.rootf[k][1] = (float)g.root[k][1];
-	}
+	fill_roots(g.roots);
 	auto ref_of = [&](unsigned bit) -> BitRef {
 		for(unsigned i = 0; i < K; ++i)
 			if(pass.lpos[i] == bit) return BitRef{true, i};
