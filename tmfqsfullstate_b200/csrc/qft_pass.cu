@@ -37,10 +37,12 @@ namespace tqb {
 
 namespace {
 
-constexpr unsigned kQftMaxThreads = 256;
 constexpr unsigned kQftMaxStages = 4;
 constexpr unsigned kQftMaxRuns = 8;
-constexpr unsigned kQftGranules = 16;  // 16-byte granules per thread per tile
+
+// Threads per CTA: 2^(K - RB) for tiles of 2^K amplitudes, at most 512 for
+// complex64 with 4 register bits (tiles of 2^13), else 256.
+constexpr unsigned qft_max_threads(size_t vbytes, int RB) { return vbytes == 8 && RB == 4 ? 512u : 256u; }
 constexpr uint32_t kQftNone = 0xffffffffu;
 
 struct QftStage {
@@ -144,32 +146,40 @@ __device__ __forceinline__ uint64_t qft_tile_base(const QftGeom &g, uint64_t o) 
 
 // v[r] times prod_{i < D, r_i = 1} f[i] (the filler bits D.. carry no factor),
 // and the real scale s on every value when SC.  The products come from two
-// small tables over bits 0..2 and 3..D-1: at most two complex products per
-// amplitude, few registers.
+// small tables over bits 0..2 and 3..D-1, applied one after the other (at most
+// two complex products per amplitude; only one table is live at a time).
 template <typename V, int RB, int D, bool SC>
 __device__ __forceinline__ void apply_twiddle(V (&v)[1 << RB], const V (&f)[D], typename Scalar<V>::type s) {
 	constexpr int LO = D < 3 ? D : 3, HI = D - LO;
-	V FL[1 << LO], FH[1 << HI];
+	{
+		V FL[1 << LO];
 #pragma unroll
-	for(int k = 1; k < (1 << LO); ++k) {
-		const int hb = 31 - __clz(k);
-		FL[k] = (k == (1 << hb)) ? f[hb] : vmul(FL[k ^ (1 << hb)], f[hb]);
+		for(int k = 1; k < (1 << LO); ++k) {
+			const int hb = 31 - __clz(k);
+			FL[k] = (k == (1 << hb)) ? f[hb] : vmul(FL[k ^ (1 << hb)], f[hb]);
+			if constexpr(SC) {
+				if(k == (1 << hb)) FL[k] = vscale(FL[k], s);
+			}
+		}
+#pragma unroll
+		for(int r = 0; r < (1 << RB); ++r) {
+			const int lo = r & ((1 << LO) - 1);
+			if(lo) v[r] = vmul(v[r], FL[lo]);
+			else if(SC) v[r] = vscale(v[r], s);
+		}
 	}
+	if constexpr(HI > 0) {
+		V FH[1 << HI];
 #pragma unroll
-	for(int k = 1; k < (1 << HI); ++k) {
-		const int hb = 31 - __clz(k);
-		FH[k] = (k == (1 << hb)) ? f[LO + hb] : vmul(FH[k ^ (1 << hb)], f[LO + hb]);
-	}
-	if constexpr(SC) {
+		for(int k = 1; k < (1 << HI); ++k) {
+			const int hb = 31 - __clz(k);
+			FH[k] = (k == (1 << hb)) ? f[LO + hb] : vmul(FH[k ^ (1 << hb)], f[LO + hb]);
+		}
 #pragma unroll
-		for(int k = 1; k < (1 << LO); ++k) FL[k] = vscale(FL[k], s);
-	}
-#pragma unroll
-	for(int r = 0; r < (1 << RB); ++r) {
-		const int k = r & ((1 << D) - 1), lo = k & ((1 << LO) - 1), hi = k >> LO;
-		if(lo) v[r] = vmul(v[r], FL[lo]);
-		else if(SC) v[r] = vscale(v[r], s);
-		if(hi) v[r] = vmul(v[r], FH[hi]);
+		for(int r = 0; r < (1 << RB); ++r) {
+			const int hi = (r & ((1 << D) - 1)) >> LO;
+			if(hi) v[r] = vmul(v[r], FH[hi]);
+		}
 	}
 }
 
@@ -247,17 +257,18 @@ __device__ __forceinline__ void qft_stage_dispatch(V *tile, const QftStage &S, u
 // factors per ring slot.  Everything is derived here from the geometry: the
 // launch needs no device program.
 template <typename R, int RB>
-__global__ void __launch_bounds__(kQftMaxThreads, 1)
+__global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type), RB), 1)
 	k_qft_pass(typename Vec2<R>::type *a, const __grid_constant__ QftGeom g) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	constexpr unsigned per16 = 16 / sizeof(V);
+	constexpr unsigned kGranules = (1u << RB) / per16;  // 16-byte granules per thread per tile
 	const unsigned T = 1u << g.K, tid = threadIdx.x, nthr = blockDim.x;
 	V *ring = reinterpret_cast<V *>(smem_raw);
 	V *ftab = ring + (size_t)g.slots * T;
 	V *orow = ftab + (size_t)g.nfrows * nthr;
 	QftStage *sst = reinterpret_cast<QftStage *>(orow + (size_t)g.slots * g.ot_stride);
-	uint32_t *spst = reinterpret_cast<uint32_t *>(sst + kQftMaxStages);
+	uint16_t *spst = reinterpret_cast<uint16_t *>(sst + kQftMaxStages);
 
 	if(tid < g.nstages) sst[tid] = g.st[tid];
 	const uint64_t goff = qft_scatter(g, tid * per16);
@@ -274,7 +285,7 @@ __global__ void __launch_bounds__(kQftMaxThreads, 1)
 			const V *src = a + base + goff;
 			V *dst = ring + (size_t)slot * T + psm;
 #pragma unroll
-			for(unsigned i = 0; i < kQftGranules; ++i) cp_async16(dst + i * gstep, src + i * g.istride);
+			for(unsigned i = 0; i < kGranules; ++i) cp_async16(dst + i * gstep, src + i * g.istride);
 			cp_async_commit();
 			const unsigned st = tid >> 5;
 			if((tid & 31u) == 0 && st < g.nstages && sst[st].ot != kQftNone)
@@ -295,7 +306,7 @@ __global__ void __launch_bounds__(kQftMaxThreads, 1)
 			const unsigned b = S.rsorted[i], lo = jt & ((1u << b) - 1u);
 			jt = ((jt ^ lo) << 1) | lo;
 		}
-		spst[st * nthr + tid] = qft_phys(g, jt);
+		spst[st * nthr + tid] = (uint16_t)qft_phys(g, jt);
 		if(S.fl != kQftNone) stage_factors<V>(qft_scatter(g, jt) & S.wmask, S.bhi, S.d, ftab + (size_t)S.fl * nthr + tid, nthr);
 	}
 
@@ -317,7 +328,7 @@ __global__ void __launch_bounds__(kQftMaxThreads, 1)
 		V *dst = a + qft_tile_base(g, o) + goff;
 		const V *src = tile + psm;
 #pragma unroll
-		for(unsigned i = 0; i < kQftGranules; ++i)
+		for(unsigned i = 0; i < kGranules; ++i)
 			*reinterpret_cast<float4 *>(dst + i * g.istride) = *reinterpret_cast<const float4 *>(src + i * gstep);
 		slot = slot + 1 == g.slots ? 0 : slot + 1;
 	}
@@ -389,14 +400,14 @@ struct Swizzle {
 };
 
 // Plans the pass for storage values of vbytes bytes and RB register bits.
-bool plan_qft(const FusedPass &pass, unsigned vbytes, unsigned RB, QftGeom &g) {
-	std::vector<unsigned> hb;
-	unsigned r0 = 0;
-	if(!qft_segment(pass, hb, r0)) return false;
+bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r0, unsigned vbytes, unsigned RB,
+              QftGeom &g) {
 	const unsigned K = pass.K, n = pass.n, per16 = 16 / vbytes;
-	if(K < RB + 5 || K - RB > 8 || K < 4) return false;
-	if(pass.lpos[K - 1] - pass.lpos[K - 4] != 3) return false;  // the granule index bits are contiguous
-	if(per16 == 2 && pass.lpos[0] != 0) return false;            // two adjacent amplitudes per granule
+	const unsigned lgran = RB - (per16 == 2 ? 1u : 0u);  // log2 of the granules per thread
+	if(K > 14 || K < RB + 5 || (1u << (K - RB)) > qft_max_threads(vbytes, (int)RB)) return false;
+	// The granule index bits (the top lgran local bits) are contiguous.
+	if(pass.lpos[K - 1] - pass.lpos[K - lgran] != lgran - 1) return false;
+	if(per16 == 2 && pass.lpos[0] != 0) return false;  // two adjacent amplitudes per granule
 	auto li = [&](unsigned bit) -> int {
 		for(unsigned i = 0; i < K; ++i)
 			if(pass.lpos[i] == bit) return (int)i;
@@ -408,7 +419,7 @@ bool plan_qft(const FusedPass &pass, unsigned vbytes, unsigned RB, QftGeom &g) {
 	g.K = K;
 	g.nstages = nst;
 	g.ntiles = 1ull << (n - K);
-	g.istride = 1ull << pass.lpos[K - 4];
+	g.istride = 1ull << pass.lpos[K - lgran];
 	for(unsigned i = 0; i < K; ++i) {
 		g.lpos[i] = pass.lpos[i];
 		g.localmask |= 1ull << pass.lpos[i];
@@ -474,7 +485,9 @@ bool plan_qft(const FusedPass &pass, unsigned vbytes, unsigned RB, QftGeom &g) {
 	// chosen so that each stage's half-warps (quarter-warps for 16-byte
 	// amplitudes) hit as few banks twice as the layout allows.
 	const unsigned bank_mask = per16 == 2 ? 15u : 7u, group = per16 == 2 ? 16u : 8u;
-	const unsigned dst0 = per16 == 2 ? 1u : 0u, src_lo = per16 == 2 ? 4u : 3u, src_hi = K - 5;
+	// The copies' thread bits are shared index bits [log2(per16), log2(per16) + K - RB).
+	const unsigned dst0 = per16 == 2 ? 1u : 0u, src_lo = per16 == 2 ? 4u : 3u;
+	const unsigned src_hi = (per16 == 2 ? 1u : 0u) + (K - RB) - 1u;
 	auto cost = [&](const Swizzle &w) {
 		unsigned total = 0;
 		for(unsigned s = 0; s < nst; ++s) {
@@ -534,15 +547,15 @@ bool plan_qft(const FusedPass &pass, unsigned vbytes, unsigned RB, QftGeom &g) {
 }
 
 template <typename R, int RB>
-bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass) {
+bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r0) {
 	typedef typename Vec2<R>::type V;
 	QftGeom g;
-	if(!plan_qft(pass, (unsigned)sizeof(V), (unsigned)RB, g)) return false;
+	if(!plan_qft(pass, hb, r0, (unsigned)sizeof(V), (unsigned)RB, g)) return false;
 	const unsigned nthr = 1u << (g.K - RB);
 	const size_t T = size_t(1) << g.K;
 	auto smem_for = [&](unsigned slots) {
 		return (slots * T + (size_t)g.nfrows * nthr + (size_t)slots * g.ot_stride) * sizeof(V) +
-		       kQftMaxStages * sizeof(QftStage) + (size_t)g.nstages * nthr * 4;
+		       kQftMaxStages * sizeof(QftStage) + (size_t)g.nstages * nthr * 2;
 	};
 	int dev = 0, max_optin = 0;
 	check_cuda(cudaGetDevice(&dev), "qft device");
@@ -561,8 +574,15 @@ bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass) {
 }  // namespace
 
 bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass) {
-	if(prec == TMFQS_FP64) return run_qft<double, 4>(c, a, pass);
-	return run_qft<float, 5>(c, a, pass);
+	std::vector<unsigned> hb;
+	unsigned r0 = 0;
+	if(!qft_segment(pass, hb, r0)) return false;
+	if(prec == TMFQS_FP64) return run_qft<double, 4>(c, a, pass, hb, r0);
+	// complex64: 4-bit stages (512 threads, more warps to hide latency) when
+	// they take no more stages than 5-bit ones.
+	const unsigned np = (unsigned)hb.size();
+	if((np + 3) / 4 == (np + 4) / 5 && run_qft<float, 4>(c, a, pass, hb, r0)) return true;
+	return run_qft<float, 5>(c, a, pass, hb, r0);
 }
 
 }  // namespace tqb
