@@ -16,10 +16,12 @@ between steps.
           loads the input from pinned host memory, runs the QFT, and reads
           back the exact total probability and a seeded measurement.
   forms   the same QFT in the two fast forms on the same GPU, device-resident:
-          complex64 (radix passes, FP64 twiddles rounded once) and complex128
-          with TMFQS_OPT_EXACT=0; each with its amp-updates/s, the HBM
-          fraction of its passes, and its accuracy against the plain result
-          (relative L2 error, fidelity, measured index).
+          complex64 (QFT segment passes k_qft_pass, FP64 twiddles rounded
+          once) and complex128 with TMFQS_OPT_EXACT=0; each with its
+          amp-updates/s, the HBM fraction of its passes, and its accuracy
+          against the plain result (relative L2 error, fidelity, measured
+          index); and complex64 again on the general radix pass
+          (TMFQS_OPT_QFT_PASS=0) for comparison.
   adjoint the differentiation form (24 qubits, 20 layers of H + ring
           controlled phases, 480 angles, E = sum_q <Z_q Z_{q+1}>): complex64
           forward and adjoint backward with a checkpoint every 48 ops; grad/s,
@@ -193,12 +195,13 @@ def pass_roofline(kt, name, peak):
             "achieved_gbs": achieved, "frac": achieved / peak}
 
 
-def run_form(tq, torch, n, inp, ops, prec, exact, steps, peak, plain, rnd, device):
+def run_form(tq, torch, n, inp, ops, prec, exact, steps, peak, plain, rnd, device, qft_pass=True):
     """One fast form of the QFT on the same input: device-resident timing and accuracy."""
     import numpy as np
 
     g = tq.GpuState(prec, device)
     g.set_option(tq.OPT_EXACT, 1 if exact else 0)
+    g.set_option(tq.OPT_QFT_PASS, 1 if qft_pass else 0)
     stream = torch.cuda.ExternalStream(g.stream())
     g.load(n, inp)
     g.apply_ops(ops)  # warm-up
@@ -216,6 +219,7 @@ def run_form(tq, torch, n, inp, ops, prec, exact, steps, peak, plain, rnd, devic
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
         kts.append(g.kernel_times())
+        qft_passes = g.stats()["qft_passes"]
         g.set_option(tq.OPT_KERNEL_TIMING, 0)
     best = min(range(steps), key=lambda i: ms[i])
     kt = kts[best]
@@ -232,7 +236,7 @@ def run_form(tq, torch, n, inp, ops, prec, exact, steps, peak, plain, rnd, devic
     return {"ms_per_qft": t, "value": len(ops) * (1 << n) / (t / 1e3), "unit": UNIT,
             "hbm_frac_whole_qft": passes * sweep / (t / 1e3) / 1e9 / peak,
             "sweeps": passes, "fused_pass": pass_roofline(kt, "fused", peak),
-            "permute_pass": pass_roofline(kt, "permute", peak),
+            "permute_pass": pass_roofline(kt, "permute", peak), "qft_segment_passes": qft_passes,
             "rel_l2_vs_plain": rel, "fidelity_vs_plain": float(fid), "measured": measured}
 
 
@@ -549,9 +553,10 @@ def run_ours(args):
     if rank == 0 and not args.no_forms:
         plain = g.export()
         forms = {}
-        for name, prec, exact in (("complex64_radix", tq.FP32, True), ("complex128_fast", tq.FP64, False)):
+        for name, prec, exact, qp in (("complex64_radix", tq.FP32, True, True), ("complex128_fast", tq.FP64, False, True),
+                                      ("complex64_general_radix", tq.FP32, True, False)):
             forms[name] = run_form(tq, torch, n, inp, ops, prec, exact, max(1, args.form_steps), peak, plain, rnd,
-                                   local)
+                                   local, qp)
             forms[name]["speedup_vs_plain"] = (ms_per_step / forms[name]["ms_per_qft"])
         del plain
 

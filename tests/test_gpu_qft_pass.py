@@ -90,6 +90,50 @@ def test_qft_pass_narrow_passes(prec, fq):
     check(n, tq.random_phase(n, 11 * fq), tq.qft_ops(n), prec, fused_qubits=fq)
 
 
+def run_chunks(n, amps, ops, prec, chunk):
+    with tq.GpuState(prec) as g:
+        g.set_option(tq.OPT_EXACT, 0)
+        g.load(n, amps)
+        for i in range(0, len(ops), chunk):
+            g.apply_ops(ops[i:i + chunk])
+        return g.export(), g.stats()
+
+
+@pytest.mark.parametrize("prec", [tq.FP64, tq.FP32])
+@pytest.mark.parametrize("chunk", [3, 7, 16])
+def test_hadamard_runs_are_not_qft_segments(prec, chunk):
+    # Runs of Hadamards on consecutive qubits without their phases (Hadamard
+    # layers, cut into pieces) are not QFT segments: the compiled ladders would
+    # add phases the circuit does not have.
+    n = 12
+    rng = np.random.default_rng(chunk)
+    a = rng.standard_normal(2 << n)
+    a /= np.linalg.norm(a)
+    th = tq.random_angles(3 * n, 9)
+    ops = tq.layered_cphase_ops(n, th)
+    got, _ = run_chunks(n, a, ops, prec, chunk)
+    assert O.rel_l2(oracle(n, a, ops), got) <= TOL[prec]
+    layer = [tq.h(q) for q in range(n)]
+    got, st = run_chunks(n, a, layer, prec, chunk)
+    assert st["qft_passes"] == 0
+    assert O.rel_l2(oracle(n, a, layer), got) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", [tq.FP64, tq.FP32])
+def test_truncated_ladder_is_not_a_segment(prec):
+    # The approximate QFT (phases only between qubits at most 3 apart): its
+    # chains stop short of a common lowest bit.
+    n = 14
+    ops = []
+    for t in range(n):
+        ops.append(tq.h(t))
+        for c in range(t + 1, min(n, t + 4)):
+            ops.append(tq.cphase(c, t, np.pi / float(1 << (c - t))))
+    amps = tq.random_phase(n, 77)
+    got, st = run_gpu(n, amps, ops, prec)
+    assert O.rel_l2(oracle(n, amps, ops), got) <= TOL[prec]
+
+
 @pytest.mark.parametrize("prec", [tq.FP64, tq.FP32])
 def test_qft_pass_twice(prec):
     n = 18

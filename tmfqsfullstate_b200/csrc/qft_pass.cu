@@ -340,7 +340,10 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 
 // Hadamards on consecutive descending bits hb[0] > hb[1] > ..., each followed
 // by the controlled phases pi/2^(b-c) with every bit c in [r0, b) (in any
-// order), and nothing else.  r0 = n when the segment has no phases.
+// order), and nothing else.  The compiled ladders apply the phases between the
+// segment's own bits, so every Hadamard above the lowest must carry its chain
+// and the lowest Hadamard bit is r0 or above (its own chain may be empty only
+// when it sits at r0).  A lone Hadamard (no phases at all) is a segment too.
 bool qft_segment(const FusedPass &pass, std::vector<unsigned> &hb, unsigned &r0) {
 	hb.clear();
 	r0 = pass.n;
@@ -349,6 +352,7 @@ bool qft_segment(const FusedPass &pass, std::vector<unsigned> &hb, unsigned &r0)
 	for(const FusedOp &f : pass.ops) {
 		if(f.kind != kFH && f.kind != kFHChain && f.kind != kFHTwiddle) return false;
 		if(f.lt >= pass.K) return false;
+		if(bare) return false;  // only the lowest Hadamard may lack phases
 		const unsigned b = pass.lpos[f.lt];
 		if(!hb.empty() && b + 1 != hb.back()) return false;
 		const unsigned cnt = f.kind == kFH ? 0u : f.lc;
@@ -365,7 +369,6 @@ bool qft_segment(const FusedPass &pass, std::vector<unsigned> &hb, unsigned &r0)
 		}
 		if(cnt != b - lo) return false;  // the phases cover [lo, b) exactly
 		if(cnt) {
-			if(bare) return false;  // an earlier, higher Hadamard lacked its phases
 			if(!have_r0) {
 				r0 = lo;
 				have_r0 = true;
@@ -373,12 +376,14 @@ bool qft_segment(const FusedPass &pass, std::vector<unsigned> &hb, unsigned &r0)
 				return false;
 			}
 		} else {
-			if(have_r0 && b > r0) return false;
-			if(!have_r0) bare = true;
+			bare = true;
 		}
 		hb.push_back(b);
 	}
-	return !hb.empty();
+	if(hb.empty()) return false;
+	if(!have_r0) return hb.size() == 1;  // Hadamards without phases: only a lone one
+	if(bare && hb.back() != r0) return false;
+	return hb.back() >= r0;
 }
 
 inline unsigned insert_zeros(unsigned t, const uint32_t *sorted, int count) {
