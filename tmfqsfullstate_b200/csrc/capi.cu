@@ -292,6 +292,9 @@ struct Planner {
 	int chain_op = -1;   // index of the H-chain op that may still grow
 	size_t nontrivial = 0;
 	std::vector<const tmfqs_op *> pending;  // circuit ops in the pass (for single-op fallback)
+	std::vector<unsigned> msched;  // fast forms: low-bit width of the first multi-op passes
+	unsigned mrest = 0;            // ... and of the passes after them
+	size_t npass = 0;              // multi-op passes run so far
 
 	explicit Planner(tmfqs_gpu_state *hh) : h(hh) {
 		// Tiles of 2^12 complex128 / 2^13 complex64 amplitudes (64 KB).  The
@@ -311,6 +314,20 @@ struct Planner {
 			mlow = mmin;
 			for(unsigned m = mmin + 1; m <= mmax; ++m)
 				if(passes(m) == passes(mmin)) mlow = m;
+			mrest = mlow;
+			// Per pass: the fewest passes need (P-1)(Kmax-mmin)+Kmax >= n bits; the
+			// spare bits widen the rows of the first passes one by one (a QFT's
+			// last pass holds the Kmax lowest bits, contiguous whatever its width).
+			if(h->opt_fused_qubits == 0 && h->n > Kmax) {
+				const unsigned P = passes(mmin);
+				unsigned slack = (P - 1) * (Kmax - mmin) + Kmax - h->n;
+				for(unsigned i = 0; i + 1 < P; ++i) {
+					const unsigned inc = std::min(mmax - mmin, slack);
+					msched.push_back(mmin + inc);
+					slack -= inc;
+				}
+				mlow = msched[0];
+			}
 		} else {
 			mlow = h->precision == TMFQS_FP64 ? 3u : 4u;
 		}
@@ -320,6 +337,7 @@ struct Planner {
 	}
 
 	void reset() {
+		if(!msched.empty()) mlow = npass < msched.size() ? msched[npass] : mrest;
 		pass = tqb::FusedPass{};
 		pass.n = h->n;
 		tmask = 0;
@@ -393,6 +411,7 @@ struct Planner {
 				}
 			}
 			pass.gate_count = (unsigned)pending.size();
+			++npass;
 			PassTimer timer(h, TMFQS_KT_FUSED, sweep_bytes(h));
 			const bool qft = twiddle && h->opt_radix && h->opt_qft_pass &&
 			                 tqb::launch_qft_pass(ctx(h), h->precision, h->amps, pass);
