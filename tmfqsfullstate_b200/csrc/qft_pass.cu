@@ -52,9 +52,10 @@ struct QftStage {
 	uint32_t roff[5];     // swizzled shared-memory offset (elements) of register bit i
 	uint32_t fl;          // first per-thread factor row, kQftNone: no twiddle
 	uint32_t ot;          // first per-tile factor in a factor row, kQftNone: none
-	uint32_t scaled;      // the pass's real scale (1/sqrt(2))^P is applied here
-	uint32_t pad;
+	uint32_t scaled;      // the pass's real scale (1/sqrt(2))^P is applied here (the last stage)
+	uint32_t direct;      // last stage: results go straight to HBM (lanes run along >= 64-byte rows)
 	uint64_t wmask;       // the bits of W: [r0, lowest Hadamard bit of the stage)
+	uint64_t gstride[5];  // global element offset of register bit i
 };
 
 struct QftGeom {
@@ -187,7 +188,7 @@ __device__ __forceinline__ void apply_twiddle(V (&v)[1 << RB], const V (&f)[D], 
 // read, transformed (ladder, twiddle, scale) and written back in place.
 template <typename V, int RB, int D, bool TW, bool SC>
 __device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
-                                              const V *ot, typename Scalar<V>::type s, const RootTable &roots) {
+                                              const V *ot, typename Scalar<V>::type s, const RootTable &roots, V *gdst) {
 	unsigned roff[RB];
 #pragma unroll
 	for(int i = 0; i < RB; ++i) roff[i] = S.roff[i];
@@ -215,6 +216,21 @@ __device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsign
 #pragma unroll
 		for(int r = 0; r < (1 << RB); ++r) v[r] = vscale(v[r], s);
 	}
+	if(SC && gdst) {
+		// The last stage's lanes run along the low index bits: coalesced rows.
+		uint64_t gs[RB];
+#pragma unroll
+		for(int i = 0; i < RB; ++i) gs[i] = S.gstride[i];
+#pragma unroll
+		for(int r = 0; r < (1 << RB); ++r) {
+			uint64_t x = 0;
+#pragma unroll
+			for(int i = 0; i < RB; ++i)
+				if((r >> i) & 1) x += gs[i];
+			gdst[x] = v[r];
+		}
+		return;
+	}
 #pragma unroll
 	for(int r = 0; r < (1 << RB); ++r) {
 		unsigned x = pbase;
@@ -227,26 +243,27 @@ __device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsign
 
 template <typename V, int RB, int D>
 __device__ __forceinline__ void qft_stage_flags(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
-                                                const V *ot, typename Scalar<V>::type s, const RootTable &roots) {
+                                                const V *ot, typename Scalar<V>::type s, const RootTable &roots, V *gdst) {
 	const bool tw = S.fl != kQftNone;
 	if(tw) {
-		if(S.scaled) qft_stage_run<V, RB, D, true, true>(tile, S, pbase, frow, nthr, ot, s, roots);
-		else qft_stage_run<V, RB, D, true, false>(tile, S, pbase, frow, nthr, ot, s, roots);
+		if(S.scaled) qft_stage_run<V, RB, D, true, true>(tile, S, pbase, frow, nthr, ot, s, roots, gdst);
+		else qft_stage_run<V, RB, D, true, false>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
 	} else {
-		if(S.scaled) qft_stage_run<V, RB, D, false, true>(tile, S, pbase, frow, nthr, ot, s, roots);
-		else qft_stage_run<V, RB, D, false, false>(tile, S, pbase, frow, nthr, ot, s, roots);
+		if(S.scaled) qft_stage_run<V, RB, D, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, gdst);
+		else qft_stage_run<V, RB, D, false, false>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
 	}
 }
 
 template <typename V, int RB>
 __device__ __forceinline__ void qft_stage_dispatch(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
-                                                   const V *ot, typename Scalar<V>::type s, const RootTable &roots) {
+                                                   const V *ot, typename Scalar<V>::type s, const RootTable &roots,
+                                                   V *gdst) {
 	switch(S.d) {
-		case 1: qft_stage_flags<V, RB, 1>(tile, S, pbase, frow, nthr, ot, s, roots); break;
-		case 2: qft_stage_flags<V, RB, 2>(tile, S, pbase, frow, nthr, ot, s, roots); break;
-		case 3: qft_stage_flags<V, RB, 3>(tile, S, pbase, frow, nthr, ot, s, roots); break;
-		case 4: qft_stage_flags<V, RB, 4>(tile, S, pbase, frow, nthr, ot, s, roots); break;
-		case 5: if constexpr(RB >= 5) qft_stage_flags<V, RB, 5>(tile, S, pbase, frow, nthr, ot, s, roots); break;
+		case 1: qft_stage_flags<V, RB, 1>(tile, S, pbase, frow, nthr, ot, s, roots, gdst); break;
+		case 2: qft_stage_flags<V, RB, 2>(tile, S, pbase, frow, nthr, ot, s, roots, gdst); break;
+		case 3: qft_stage_flags<V, RB, 3>(tile, S, pbase, frow, nthr, ot, s, roots, gdst); break;
+		case 4: qft_stage_flags<V, RB, 4>(tile, S, pbase, frow, nthr, ot, s, roots, gdst); break;
+		case 5: if constexpr(RB >= 5) qft_stage_flags<V, RB, 5>(tile, S, pbase, frow, nthr, ot, s, roots, gdst); break;
 		default: break;
 	}
 }
@@ -298,7 +315,9 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 	uint64_t o = blockIdx.x;
 	for(unsigned k = 0; k + 1 < g.slots; ++k) prefetch(o + (uint64_t)k * gridDim.x, k);
 
-	// Per-thread tables (once per launch).
+	// Per-thread tables (once per launch), and the global offset of the
+	// thread's first amplitude in the last stage (direct stores).
+	uint64_t slast = 0;
 	for(unsigned st = 0; st < g.nstages; ++st) {
 		const QftStage &S = sst[st];
 		unsigned jt = tid;
@@ -308,7 +327,9 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 		}
 		spst[st * nthr + tid] = (uint16_t)qft_phys(g, jt);
 		if(S.fl != kQftNone) stage_factors<V>(qft_scatter(g, jt) & S.wmask, S.bhi, S.d, ftab + (size_t)S.fl * nthr + tid, nthr);
+		if(st + 1 == g.nstages) slast = qft_scatter(g, jt);
 	}
+	const bool direct = sst[g.nstages - 1].direct != 0;
 
 	const typename Scalar<V>::type s = (typename Scalar<V>::type)g.scale;
 	unsigned slot = 0;
@@ -319,17 +340,23 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 		prefetch(o + (uint64_t)(g.slots - 1) * gridDim.x, slot == 0 ? g.slots - 1 : slot - 1);
 		V *tile = ring + (size_t)slot * T;
 		const V *ot = orow + slot * g.ot_stride;
+		const uint64_t tbase = qft_tile_base(g, o);
 		for(unsigned st = 0; st < g.nstages; ++st) {
 			const QftStage &S = sst[st];
 			const V *frow = ftab + (size_t)(S.fl == kQftNone ? 0u : S.fl) * nthr + tid;
-			qft_stage_dispatch<V, RB>(tile, S, spst[st * nthr + tid], frow, nthr, ot, s, g.roots);
-			__syncthreads();
+			const bool last = st + 1 == g.nstages;
+			qft_stage_dispatch<V, RB>(tile, S, spst[st * nthr + tid], frow, nthr, ot, s, g.roots,
+			                          last && direct ? a + tbase + slast : nullptr);
+			// After a direct last stage the next tile's first barrier protects the buffer.
+			if(!(last && direct)) __syncthreads();
 		}
-		V *dst = a + qft_tile_base(g, o) + goff;
-		const V *src = tile + psm;
+		if(!direct) {
+			V *dst = a + tbase + goff;
+			const V *src = tile + psm;
 #pragma unroll
-		for(unsigned i = 0; i < kGranules; ++i)
-			*reinterpret_cast<float4 *>(dst + i * g.istride) = *reinterpret_cast<const float4 *>(src + i * gstep);
+			for(unsigned i = 0; i < kGranules; ++i)
+				*reinterpret_cast<float4 *>(dst + i * g.istride) = *reinterpret_cast<const float4 *>(src + i * gstep);
+		}
 		slot = slot + 1 == g.slots ? 0 : slot + 1;
 	}
 	cp_async_wait_all();
@@ -481,6 +508,16 @@ bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r
 			}
 		}
 		S.scaled = s + 1 == nst;
+		for(unsigned i = 0; i < RB; ++i) S.gstride[i] = 1ull << pass.lpos[rbit[s][i]];
+		// Direct stores from the last stage when its lanes start with the lowest
+		// contiguous index bits: rows of at least 64 bytes per warp store.
+		if(S.scaled) {
+			const unsigned need = vbytes == 8 ? 3u : 2u;
+			bool ok = true;
+			for(unsigned l = 0; l < need; ++l)
+				if(l >= K || pass.lpos[l] != l || ((used >> l) & 1u)) ok = false;
+			S.direct = ok;
+		}
 	}
 	g.nfrows = nfrows;
 	g.ot_stride = ocol;
