@@ -59,7 +59,18 @@ struct DeviceScope {
 	explicit DeviceScope(const tmfqs_gpu_state *h) { check_cuda(cudaSetDevice(h->device), "cudaSetDevice"); }
 };
 
-tqb::LaunchCtx ctx(tmfqs_gpu_state *h) { return tqb::LaunchCtx{h->stream, h->num_sms, &h->stats.kernel_launches}; }
+tqb::LaunchCtx ctx(tmfqs_gpu_state *h) {
+	return tqb::LaunchCtx{h->stream, h->num_sms, &h->stats.kernel_launches, h->err_dev};
+}
+
+// Reports (and clears) a failure recorded by a bounded device wait since the
+// last check.  Call after the stream has been synchronized.
+void check_device_error(tmfqs_gpu_state *h) {
+	if(h->err_host && *reinterpret_cast<volatile int *>(h->err_host)) {
+		*reinterpret_cast<volatile int *>(h->err_host) = 0;
+		fail(TMFQS_ERR_RUNTIME, "a device pass gave up waiting for its tile copies");
+	}
+}
 
 size_t amp_bytes(const tmfqs_gpu_state *h) { return h->precision == TMFQS_FP64 ? 16 : 8; }
 
@@ -986,6 +997,7 @@ void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count) {
 		throw;
 	}
 	check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
+	check_device_error(h);
 }
 
 // ---- adjoint gradient (tmfqs_gpu_adjoint_gradient) ----
@@ -1192,7 +1204,15 @@ int tmfqs_gpu_create(int precision, int device, tmfqs_gpu_state **out) {
 				fail(TMFQS_ERR_NOMEM, "pinned staging allocation failed");
 			}
 			h->pinned_elems = kPinnedElems;
+			if(cudaHostAlloc(&h->err_host, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+			   cudaHostGetDevicePointer(&h->err_dev, h->err_host, 0) != cudaSuccess) {
+				cudaGetLastError();
+				fail(TMFQS_ERR_NOMEM, "pinned error word allocation failed");
+			}
+			*h->err_host = 0;
 		} catch(...) {
+			if(h->err_host) cudaFreeHost(h->err_host);
+			if(h->pinned) cudaFreeHost(h->pinned);
 			if(h->stream) cudaStreamDestroy(h->stream);
 			delete h;
 			throw;
@@ -1217,6 +1237,7 @@ int tmfqs_gpu_destroy(tmfqs_gpu_state *h) {
 		if(h->dev_small) cudaFree(h->dev_small);
 		if(h->dev_prog) cudaFree(h->dev_prog);
 		if(h->pinned) cudaFreeHost(h->pinned);
+		if(h->err_host) cudaFreeHost(h->err_host);
 		if(h->stream) cudaStreamDestroy(h->stream);
 		delete h;
 	});

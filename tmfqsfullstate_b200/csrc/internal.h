@@ -70,6 +70,7 @@ struct LaunchCtx {
 	cudaStream_t stream;
 	int num_sms;
 	uint64_t *launches;
+	int *err = nullptr;  // device-visible error word of the handle (nonzero: a bounded wait gave up)
 };
 
 void launch_h(const LaunchCtx &c, int prec, void *a, unsigned n, unsigned bit);
@@ -257,6 +258,8 @@ struct tmfqs_gpu_state {
 	bool opt_radix = true;  // fast forms: radix passes where the program allows
 	bool opt_tensor = true; // complex64: 4- and 5-qubit gates on the tensor cores
 	bool opt_qft_pass = true;  // fast forms: QFT ladder segments on the dedicated QFT pass
+	int *err_host = nullptr;   // mapped pinned error word written by bounded device waits
+	int *err_dev = nullptr;
 	void *dev_tc = nullptr; // tensor-core gate operands
 	size_t dev_tc_bytes = 0;
 	// Adjoint-gradient work buffers, kept for the next call (freed by destroy):

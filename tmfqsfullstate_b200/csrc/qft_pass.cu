@@ -268,6 +268,34 @@ __device__ __forceinline__ void qft_stage_dispatch(V *tile, const QftStage &S, u
 	}
 }
 
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count) {
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+
+// Arrives on the barrier once this thread's earlier cp.async copies are done
+// (the barrier's count includes this arrival: .noinc).
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *b) {
+	asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *b, unsigned parity) {
+	uint32_t ok;
+	asm volatile(
+		"{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.b32 %0, 1, 0, p;\n\t}"
+		: "=r"(ok)
+		: "r"(smem_u32(b)), "r"(parity)
+		: "memory");
+	return ok != 0;
+}
+
+// Upper bound on the polls of a tile's arrival (each poll may suspend the
+// thread for a while).  Past it the thread records the failure in the
+// handle's error word and goes on (every thread keeps the same barrier
+// sequence; the host reports the error after the pass).
+constexpr int kQftWaitPolls = 1 << 22;
+
 // The pass.  Shared memory: the ring of tile buffers, the stage descriptors,
 // the per-thread twiddle factors [nfrows][nthr], the swizzled index of each
 // thread's first amplitude per stage [nstages][nthr], and one row of per-tile
@@ -275,7 +303,7 @@ __device__ __forceinline__ void qft_stage_dispatch(V *tile, const QftStage &S, u
 // launch needs no device program.
 template <typename R, int RB>
 __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type), RB), 1)
-	k_qft_pass(typename Vec2<R>::type *a, const __grid_constant__ QftGeom g) {
+	k_qft_pass(typename Vec2<R>::type *a, const __grid_constant__ QftGeom g, int *err) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	constexpr unsigned per16 = 16 / sizeof(V);
@@ -285,9 +313,12 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 	V *ftab = ring + (size_t)g.slots * T;
 	V *orow = ftab + (size_t)g.nfrows * nthr;
 	QftStage *sst = reinterpret_cast<QftStage *>(orow + (size_t)g.slots * g.ot_stride);
-	uint16_t *spst = reinterpret_cast<uint16_t *>(sst + kQftMaxStages);
+	uint64_t *mbar = reinterpret_cast<uint64_t *>(sst + kQftMaxStages);  // [slots]: arrival of each slot's tile
+	uint16_t *spst = reinterpret_cast<uint16_t *>(mbar + g.slots);
 
 	if(tid < g.nstages) sst[tid] = g.st[tid];
+	if(tid == 0)
+		for(unsigned k = 0; k < g.slots; ++k) mbar_init(&mbar[k], nthr);
 	const uint64_t goff = qft_scatter(g, tid * per16);
 	const unsigned psm = qft_phys(g, tid * per16);
 	const unsigned gstep = nthr * per16;  // shared index step between a thread's granules
@@ -303,13 +334,11 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 			V *dst = ring + (size_t)slot * T + psm;
 #pragma unroll
 			for(unsigned i = 0; i < kGranules; ++i) cp_async16(dst + i * gstep, src + i * g.istride);
-			cp_async_commit();
+			cp_async_mbar_arrive(&mbar[slot]);
 			const unsigned st = tid >> 5;
 			if((tid & 31u) == 0 && st < g.nstages && sst[st].ot != kQftNone)
 				stage_factors<V>(base & sst[st].wmask & ~g.localmask, sst[st].bhi, sst[st].d,
 				                 orow + slot * g.ot_stride + sst[st].ot, 1);
-		} else {
-			cp_async_commit();
 		}
 	};
 	uint64_t o = blockIdx.x;
@@ -332,12 +361,14 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 	const bool direct = sst[g.nstages - 1].direct != 0;
 
 	const typename Scalar<V>::type s = (typename Scalar<V>::type)g.scale;
-	unsigned slot = 0;
+	__syncthreads();  // tables and barrier initialisation visible
+	unsigned slot = 0, phase = 0;
 	for(; o < g.ntiles; o += gridDim.x) {
-		if(g.slots == 3) cp_async_wait1();
-		else cp_async_wait_all();
-		__syncthreads();
-		prefetch(o + (uint64_t)(g.slots - 1) * gridDim.x, slot == 0 ? g.slots - 1 : slot - 1);
+		// The tile's copies (every thread's) are done once the slot's barrier
+		// completes this phase.
+		bool ready = false;
+		for(int it = 0; it < kQftWaitPolls && !ready; ++it) ready = mbar_try_wait(&mbar[slot], phase);
+		if(!ready) atomicExch(err, 1);
 		V *tile = ring + (size_t)slot * T;
 		const V *ot = orow + slot * g.ot_stride;
 		const uint64_t tbase = qft_tile_base(g, o);
@@ -347,8 +378,14 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 			const bool last = st + 1 == g.nstages;
 			qft_stage_dispatch<V, RB>(tile, S, spst[st * nthr + tid], frow, nthr, ot, s, g.roots,
 			                          last && direct ? a + tbase + slast : nullptr);
-			// After a direct last stage the next tile's first barrier protects the buffer.
 			if(!(last && direct)) __syncthreads();
+			// Past the first stage's barrier every thread is done with the
+			// previous tile's buffer: the next copies go there.  (A pass of one
+			// direct stage has no barrier of its own: take one.)
+			if(st == 0) {
+				if(last && direct) __syncthreads();
+				prefetch(o + (uint64_t)(g.slots - 1) * gridDim.x, slot == 0 ? g.slots - 1 : slot - 1);
+			}
 		}
 		if(!direct) {
 			V *dst = a + tbase + goff;
@@ -357,7 +394,10 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 			for(unsigned i = 0; i < kGranules; ++i)
 				*reinterpret_cast<float4 *>(dst + i * g.istride) = *reinterpret_cast<const float4 *>(src + i * gstep);
 		}
-		slot = slot + 1 == g.slots ? 0 : slot + 1;
+		if(++slot == g.slots) {
+			slot = 0;
+			phase ^= 1u;
+		}
 	}
 	cp_async_wait_all();
 }
@@ -592,12 +632,12 @@ template <typename R, int RB>
 bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r0) {
 	typedef typename Vec2<R>::type V;
 	QftGeom g;
-	if(!plan_qft(pass, hb, r0, (unsigned)sizeof(V), (unsigned)RB, g)) return false;
+	if(!c.err || !plan_qft(pass, hb, r0, (unsigned)sizeof(V), (unsigned)RB, g)) return false;
 	const unsigned nthr = 1u << (g.K - RB);
 	const size_t T = size_t(1) << g.K;
 	auto smem_for = [&](unsigned slots) {
 		return (slots * T + (size_t)g.nfrows * nthr + (size_t)slots * g.ot_stride) * sizeof(V) +
-		       kQftMaxStages * sizeof(QftStage) + (size_t)g.nstages * nthr * 2;
+		       kQftMaxStages * sizeof(QftStage) + slots * 8 + (size_t)g.nstages * nthr * 2;
 	};
 	int dev = 0, max_optin = 0;
 	check_cuda(cudaGetDevice(&dev), "qft device");
@@ -607,7 +647,7 @@ bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass, const std::vect
 	if(smem > (size_t)max_optin) return false;
 	check_cuda(cudaFuncSetAttribute(k_qft_pass<R, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "qft smem");
 	const uint64_t grid = std::min<uint64_t>(g.ntiles, (uint64_t)c.num_sms);
-	k_qft_pass<R, RB><<<(unsigned)grid, nthr, smem, c.stream>>>(static_cast<V *>(a), g);
+	k_qft_pass<R, RB><<<(unsigned)grid, nthr, smem, c.stream>>>(static_cast<V *>(a), g, c.err);
 	check_cuda(cudaGetLastError(), "qft pass");
 	if(c.launches) ++*c.launches;
 	return true;
