@@ -348,6 +348,7 @@ constexpr unsigned kPermMaxLocal = 12;
 constexpr unsigned kPermThreads = 256;
 constexpr unsigned kPermHalf = 6;  // index bits per lookup table
 constexpr unsigned kPermChunks = 4;  // 6-bit chunks of the tile index (up to 24 outer bits)
+constexpr unsigned kPermGranules = 4;  // 16-byte granules per thread per tile (tiles of <= 16 KB)
 
 // Local bits of a permutation tile: two tiles of 16 KB.
 template <typename R>
@@ -446,16 +447,33 @@ __global__ void __launch_bounds__(kPermThreads) k_bit_perm(typename Vec2<R>::typ
 		return Work{g.ntiles, 0, 0, 0};
 	};
 	// Global memory moves in 16-byte granules of G consecutive amplitudes
-	// (local bit 0 is global bit 0).  The swizzle keeps granules whole.
+	// (local bit 0 is global bit 0).  The swizzle keeps granules whole.  A
+	// thread's granules (q = tid + i * blockDim) and the shared slots its
+	// outputs come from are the same for every tile: mapped once, here.
 	constexpr unsigned G = 16 / sizeof(V);
 	const unsigned TG = T / G;
+	uint64_t goff[kPermGranules];
+	unsigned pslot[kPermGranules], src[kPermGranules][G];
+	bool gv[kPermGranules];
+#pragma unroll
+	for(unsigned i = 0; i < kPermGranules; ++i) {
+		const unsigned q = threadIdx.x + i * blockDim.x;
+		gv[i] = q < TG;
+		const unsigned j = gv[i] ? q * G : 0u;
+		goff[i] = scatter(j);
+		pslot[i] = phys(j);
+#pragma unroll
+		for(unsigned e = 0; e < G; ++e) src[i][e] = phys(perm(j + e));  // involution: source of slot j+e
+	}
 	auto prefetch = [&](const Work &w, V *dst) {
 		if(w.o < g.ntiles) {
-			for(unsigned q = threadIdx.x; q < TG; q += blockDim.x) {
-				const unsigned j = q * G;
-				cp_async16(dst + phys(j), a + (w.base | scatter(j)));
-				if(w.po != w.o) cp_async16(dst + T + phys(j), a + (w.pbase | scatter(j)));
-			}
+			const bool pair = w.po != w.o;
+#pragma unroll
+			for(unsigned i = 0; i < kPermGranules; ++i)
+				if(gv[i]) {
+					cp_async16(dst + pslot[i], a + (w.base | goff[i]));
+					if(pair) cp_async16(dst + T + pslot[i], a + (w.pbase | goff[i]));
+				}
 		}
 		cp_async_commit();
 	};
@@ -470,17 +488,18 @@ __global__ void __launch_bounds__(kPermThreads) k_bit_perm(typename Vec2<R>::typ
 		const V *A = buf + 2 * T * sel, *B = A + T;
 		const bool pair = cur.po != cur.o;
 		// amplitude (base|scatter(j)) moves to (pbase|scatter(perm(j))).
-		for(unsigned q = threadIdx.x; q < TG; q += blockDim.x) {
+#pragma unroll
+		for(unsigned i = 0; i < kPermGranules; ++i) {
+			if(!gv[i]) continue;
 			float4 wa, wb;
 			V *ya = reinterpret_cast<V *>(&wa), *yb = reinterpret_cast<V *>(&wb);
 #pragma unroll
 			for(unsigned e = 0; e < G; ++e) {
-				const unsigned js = phys(perm(q * G + e));  // involution: source of slot q*G+e
-				ya[e] = A[js];
-				if(pair) yb[e] = B[js];
+				ya[e] = A[src[i][e]];
+				if(pair) yb[e] = B[src[i][e]];
 			}
-			*reinterpret_cast<float4 *>(a + (cur.pbase | scatter(q * G))) = wa;
-			if(pair) *reinterpret_cast<float4 *>(a + (cur.base | scatter(q * G))) = wb;
+			*reinterpret_cast<float4 *>(a + (cur.pbase | goff[i])) = wa;
+			if(pair) *reinterpret_cast<float4 *>(a + (cur.base | goff[i])) = wb;
 		}
 		__syncthreads();
 		cur = nxt;
@@ -674,6 +693,8 @@ void run_perm(const LaunchCtx &c, void *a, unsigned n, const std::vector<std::pa
 	}
 	g.ntiles = 1ull << (n - g.K);
 	if(n - g.K > 6 * kPermChunks) fail(TMFQS_ERR_INVALID_ARGUMENT, "bit permutation: state too large");
+	if((sizeof(typename Vec2<R>::type) << g.K) > 16 * kPermGranules * kPermThreads)
+		fail(TMFQS_ERR_LOGIC, "bit permutation: tile larger than the per-thread granule maps");
 	const size_t smem = 4 * (sizeof(typename Vec2<R>::type) << g.K) + (sizeof(uint64_t) << (g.K - g.m)) +
 	                    sizeof(uint64_t) * kPermChunks * 64 * 3 + 4 * H * sizeof(uint16_t);
 	check_cuda(cudaFuncSetAttribute(k_bit_perm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "perm smem");
