@@ -40,8 +40,8 @@ namespace {
 constexpr unsigned kQftMaxStages = 4;
 constexpr unsigned kQftMaxRuns = 8;
 
-// Threads per CTA: 2^(K - RB) for tiles of 2^K amplitudes, at most 512 for
-// complex64 with 4 register bits (tiles of 2^13), else 256.
+// Threads per CTA: 2^(K - RB) for tiles of 2^K amplitudes, at most 512 (a
+// complex64 kernel with 4 register bits), else 256.
 constexpr unsigned qft_max_threads(size_t vbytes, int RB) { return vbytes == 8 && RB == 4 ? 512u : 256u; }
 constexpr uint32_t kQftNone = 0xffffffffu;
 
@@ -660,10 +660,9 @@ bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pas
 	unsigned r0 = 0;
 	if(!qft_segment(pass, hb, r0)) return false;
 	if(prec == TMFQS_FP64) return run_qft<double, 4>(c, a, pass, hb, r0);
-	// complex64: 4-bit stages (512 threads, more warps to hide latency) when
-	// they take no more stages than 5-bit ones.
-	const unsigned np = (unsigned)hb.size();
-	if((np + 3) / 4 == (np + 4) / 5 && run_qft<float, 4>(c, a, pass, hb, r0)) return true;
+	// complex64: 5-bit stages (256 threads).  4-bit stages with 512 threads
+	// measured the same at 28 and 30 qubits and 2% slower at 26 with one
+	// barrier per tile.
 	return run_qft<float, 5>(c, a, pass, hb, r0);
 }
 
