@@ -43,6 +43,9 @@ constexpr unsigned kQftMaxRuns = 8;
 // Threads per CTA: 2^(K - RB) for tiles of 2^K amplitudes, at most 512 (a
 // complex64 kernel with 4 register bits), else 256.
 constexpr unsigned qft_max_threads(size_t vbytes, int RB) { return vbytes == 8 && RB == 4 ? 512u : 256u; }
+
+// Local bits of a full-size tile (64 KiB): 13 complex64, 12 complex128.
+constexpr int qft_tile_bits(size_t vbytes) { return vbytes == 8 ? 13 : 12; }
 constexpr uint32_t kQftNone = 0xffffffffu;
 
 struct QftStage {
@@ -54,6 +57,8 @@ struct QftStage {
 	uint32_t ot;          // first per-tile factor in a factor row, kQftNone: none
 	uint32_t scaled;      // the pass's real scale (1/sqrt(2))^P is applied here (the last stage)
 	uint32_t direct;      // last stage: results go straight to HBM (lanes run along >= 64-byte rows)
+	uint32_t top;         // register bit i is local bit kTop - 1 - i (the tile's top bits), unswizzled
+	uint32_t pad1;
 	uint64_t wmask;       // the bits of W: [r0, lowest Hadamard bit of the stage)
 	uint64_t gstride[5];  // global element offset of register bit i
 };
@@ -186,20 +191,23 @@ __device__ __forceinline__ void apply_twiddle(V (&v)[1 << RB], const V (&f)[D], 
 
 // One stage on the tile in shared memory: the thread's 2^RB amplitudes are
 // read, transformed (ladder, twiddle, scale) and written back in place.
-template <typename V, int RB, int D, bool TW, bool SC>
+template <typename V, int RB, int D, bool TW, bool SC, bool TOP>
 __device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
                                               const V *ot, typename Scalar<V>::type s, const RootTable &roots, V *gdst) {
+	// TOP: the register bits are the tile's top local bits in order, so the
+	// offsets are compile-time constants added to the thread's base.
+	constexpr int kTop = qft_tile_bits(sizeof(V));
 	unsigned roff[RB];
 #pragma unroll
-	for(int i = 0; i < RB; ++i) roff[i] = S.roff[i];
+	for(int i = 0; i < RB; ++i) roff[i] = TOP ? (1u << (kTop - 1 - i)) : S.roff[i];
 	V v[1 << RB];
 #pragma unroll
 	for(int r = 0; r < (1 << RB); ++r) {
-		unsigned x = pbase;
+		unsigned x = TOP ? 0u : pbase;
 #pragma unroll
 		for(int i = 0; i < RB; ++i)
 			if((r >> i) & 1) x ^= roff[i];
-		v[r] = tile[x];
+		v[r] = TOP ? tile[pbase + x] : tile[x];
 	}
 	qft_stage<V, RB, D>(v, roots);
 	if constexpr(TW) {
@@ -233,11 +241,12 @@ __device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsign
 	}
 #pragma unroll
 	for(int r = 0; r < (1 << RB); ++r) {
-		unsigned x = pbase;
+		unsigned x = TOP ? 0u : pbase;
 #pragma unroll
 		for(int i = 0; i < RB; ++i)
 			if((r >> i) & 1) x ^= roff[i];
-		tile[x] = v[r];
+		if(TOP) tile[pbase + x] = v[r];
+		else tile[x] = v[r];
 	}
 }
 
@@ -246,11 +255,12 @@ __device__ __forceinline__ void qft_stage_flags(V *tile, const QftStage &S, unsi
                                                 const V *ot, typename Scalar<V>::type s, const RootTable &roots, V *gdst) {
 	const bool tw = S.fl != kQftNone;
 	if(tw) {
-		if(S.scaled) qft_stage_run<V, RB, D, true, true>(tile, S, pbase, frow, nthr, ot, s, roots, gdst);
-		else qft_stage_run<V, RB, D, true, false>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
+		if(S.scaled) qft_stage_run<V, RB, D, true, true, false>(tile, S, pbase, frow, nthr, ot, s, roots, gdst);
+		else if(S.top) qft_stage_run<V, RB, D, true, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
+		else qft_stage_run<V, RB, D, true, false, false>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
 	} else {
-		if(S.scaled) qft_stage_run<V, RB, D, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, gdst);
-		else qft_stage_run<V, RB, D, false, false>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
+		if(S.scaled) qft_stage_run<V, RB, D, false, true, false>(tile, S, pbase, frow, nthr, ot, s, roots, gdst);
+		else qft_stage_run<V, RB, D, false, false, false>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
 	}
 }
 
@@ -587,27 +597,36 @@ bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r
 	Swizzle best;
 	for(int k = 0; k < 3; ++k) best.dst[k] = dst0 + k;
 	unsigned best_cost = cost(best), best_used = 0;
-	for(unsigned x : cand)
-		for(unsigned y : cand)
-			for(unsigned z : cand) {
-				Swizzle w = best;
-				w.src[0] = x;
-				w.src[1] = y;
-				w.src[2] = z;
-				const unsigned used = (x != 0) + (y != 0) + (z != 0);
-				const unsigned cc = cost(w);
-				if(cc < best_cost || (cc == best_cost && used < best_used)) {
-					best = w;
-					best_cost = cc;
-					best_used = used;
+	// A cost of one wavefront group per stage is the floor: no search needed.
+	if(best_cost > nst) {
+		for(unsigned x : cand)
+			for(unsigned y : cand)
+				for(unsigned z : cand) {
+					Swizzle w = best;
+					w.src[0] = x;
+					w.src[1] = y;
+					w.src[2] = z;
+					const unsigned used = (x != 0) + (y != 0) + (z != 0);
+					const unsigned cc = cost(w);
+					if(cc < best_cost || (cc == best_cost && used < best_used)) {
+						best = w;
+						best_cost = cc;
+						best_used = used;
+					}
 				}
-			}
+	}
 	for(int k = 0; k < 3; ++k) {
 		g.sw_src[k] = best.src[k];
 		g.sw_dst[k] = best.dst[k];
 	}
-	for(unsigned s = 0; s < nst; ++s)
-		for(unsigned i = 0; i < RB; ++i) g.st[s].roff[i] = best(1u << rbit[s][i]);
+	for(unsigned s = 0; s < nst; ++s) {
+		bool top = K == (unsigned)qft_tile_bits(vbytes);
+		for(unsigned i = 0; i < RB; ++i) {
+			g.st[s].roff[i] = best(1u << rbit[s][i]);
+			if(rbit[s][i] != K - 1 - i || g.st[s].roff[i] != (1u << rbit[s][i])) top = false;
+		}
+		g.st[s].top = top;
+	}
 
 	// Runs of outer bits, ascending.
 	g.nruns = 0;
