@@ -58,7 +58,7 @@ struct QftStage {
 	uint32_t scaled;      // the pass's real scale (1/sqrt(2))^P is applied here (the last stage)
 	uint32_t direct;      // last stage: results go straight to HBM (lanes run along >= 64-byte rows)
 	uint32_t top;         // register bit i is local bit kTop - 1 - i (the tile's top bits), unswizzled
-	uint32_t pad1;
+	uint32_t tail;        // last stage on the tile's lowest bits, fused into the copy-out (qft_tail)
 	uint64_t wmask;       // the bits of W: [r0, lowest Hadamard bit of the stage)
 	uint64_t gstride[5];  // global element offset of register bit i
 };
@@ -306,6 +306,60 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *b, unsigned parity) {
 // sequence; the host reports the error after the pass).
 constexpr int kQftWaitPolls = 1 << 22;
 
+// r with its low d bits reversed (a loop, not recursion, so that it folds once
+// the callers' loops are unrolled).
+__host__ __device__ constexpr int brev_bits(int r, int d) {
+	int x = 0;
+	for(int i = 0; i < d; ++i) x |= ((r >> i) & 1) << (d - 1 - i);
+	return x;
+}
+
+// The pass's last D Hadamards when they sit on the tile's lowest bits (local
+// bits D-1..0 = global bits D-1..0, no twiddle after them), fused into the
+// copy-out: each thread takes 2^D consecutive amplitudes from shared memory,
+// applies their ladder and the pass's scale, and stores them contiguously
+// (consecutive threads take consecutive groups).  Register bit i is local bit
+// D-1-i, so register r holds element brev(r).
+template <typename V, int D>
+__device__ __forceinline__ void qft_tail(const V *tile, V *dst, unsigned T, unsigned tid, unsigned nthr, const QftGeom &g,
+                                         typename Scalar<V>::type s) {
+	constexpr unsigned E = 1u << D;
+	unsigned pe[E];
+#pragma unroll
+	for(unsigned e = 0; e < E; ++e) pe[e] = qft_phys(g, e);
+	for(unsigned q = tid; q < T / E; q += nthr) {
+		const unsigned j = q * E, pj = qft_phys(g, j);
+		V in[E];
+		if constexpr(sizeof(V) == 8) {
+			// 16-byte reads: elements e and e + 1 stay adjacent under the swizzle.
+#pragma unroll
+			for(unsigned e = 0; e < E; e += 2) {
+				const float4 t = *reinterpret_cast<const float4 *>(tile + (pj ^ pe[e]));
+				in[e] = make_float2(t.x, t.y);
+				in[e + 1] = make_float2(t.z, t.w);
+			}
+		} else {
+#pragma unroll
+			for(unsigned e = 0; e < E; ++e) in[e] = tile[pj ^ pe[e]];
+		}
+		V v[E];
+#pragma unroll
+		for(int r = 0; r < (int)E; ++r) v[r] = in[brev_bits(r, D)];
+		qft_stage<V, D, D>(v, g.roots);
+		V out[E];
+#pragma unroll
+		for(int r = 0; r < (int)E; ++r) out[brev_bits(r, D)] = vscale(v[r], s);
+		if constexpr(sizeof(V) == 8) {
+#pragma unroll
+			for(unsigned e = 0; e < E; e += 2)
+				*reinterpret_cast<float4 *>(dst + j + e) = make_float4(out[e].x, out[e].y, out[e + 1].x, out[e + 1].y);
+		} else {
+#pragma unroll
+			for(unsigned e = 0; e < E; ++e) dst[j + e] = out[e];
+		}
+	}
+}
+
 // The pass.  Shared memory: the ring of tile buffers, the stage descriptors,
 // the per-thread twiddle factors [nfrows][nthr], the swizzled index of each
 // thread's first amplitude per stage [nstages][nthr], and one row of per-tile
@@ -369,6 +423,8 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 		if(st + 1 == g.nstages) slast = qft_scatter(g, jt);
 	}
 	const bool direct = sst[g.nstages - 1].direct != 0;
+	const bool tail = sst[g.nstages - 1].tail != 0;
+	const unsigned nrun = tail ? g.nstages - 1 : g.nstages;  // stages run through shared memory
 
 	const typename Scalar<V>::type s = (typename Scalar<V>::type)g.scale;
 	__syncthreads();  // tables and barrier initialisation visible
@@ -382,7 +438,7 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 		V *tile = ring + (size_t)slot * T;
 		const V *ot = orow + slot * g.ot_stride;
 		const uint64_t tbase = qft_tile_base(g, o);
-		for(unsigned st = 0; st < g.nstages; ++st) {
+		for(unsigned st = 0; st < nrun; ++st) {
 			const QftStage &S = sst[st];
 			const V *frow = ftab + (size_t)(S.fl == kQftNone ? 0u : S.fl) * nthr + tid;
 			const bool last = st + 1 == g.nstages;
@@ -397,7 +453,14 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 				prefetch(o + (uint64_t)(g.slots - 1) * gridDim.x, slot == 0 ? g.slots - 1 : slot - 1);
 			}
 		}
-		if(!direct) {
+		if(tail) {
+			switch(sst[g.nstages - 1].d) {
+				case 1: qft_tail<V, 1>(tile, a + tbase, T, tid, nthr, g, s); break;
+				case 2: qft_tail<V, 2>(tile, a + tbase, T, tid, nthr, g, s); break;
+				case 3: qft_tail<V, 3>(tile, a + tbase, T, tid, nthr, g, s); break;
+				default: break;
+			}
+		} else if(!direct) {
 			V *dst = a + tbase + goff;
 			const V *src = tile + psm;
 #pragma unroll
@@ -572,6 +635,20 @@ bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r
 	g.nfrows = nfrows;
 	g.ot_stride = ocol;
 
+	// The last stage goes into the copy-out when it holds at most 3 Hadamards
+	// on the tile's lowest bits, the whole tile is contiguous in the state and
+	// no twiddle follows it.
+	{
+		QftStage &L = g.st[nst - 1];
+		bool contiguous = true;
+		for(unsigned l = 0; l < K; ++l)
+			if(pass.lpos[l] != l) contiguous = false;
+		if(nst >= 2 && L.d <= 3 && L.wmask == 0 && L.bhi == L.d - 1 && contiguous) {
+			L.tail = 1;
+			L.direct = 0;
+		}
+	}
+
 	// Swizzle: shared index bits dst ^= local bits src, the sources among the
 	// thread bits of the copies (so a thread's granules stay at fixed offsets),
 	// chosen so that each stage's half-warps (quarter-warps for 16-byte
@@ -580,13 +657,23 @@ bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r
 	// The copies' thread bits are shared index bits [log2(per16), log2(per16) + K - RB).
 	const unsigned dst0 = per16 == 2 ? 1u : 0u, src_lo = per16 == 2 ? 4u : 3u;
 	const unsigned src_hi = (per16 == 2 ? 1u : 0u) + (K - RB) - 1u;
+	const bool tail = g.st[nst - 1].tail != 0;
 	auto cost = [&](const Swizzle &w) {
 		unsigned total = 0;
 		for(unsigned s = 0; s < nst; ++s) {
 			unsigned count[16] = {0}, worst = 0;
-			for(unsigned lane = 0; lane < group; ++lane) {
-				const unsigned b = w(insert_zeros(lane, g.st[s].rsorted, (int)RB)) & bank_mask;
-				worst = std::max(worst, ++count[b]);
+			if(tail && s + 1 == nst) {
+				// The fused tail: lane q reads the 16-byte granule at q * 2^d
+				// (a quarter-warp per wavefront).
+				for(unsigned lane = 0; lane < 8; ++lane) {
+					const unsigned b = (w(lane << g.st[s].d) >> (per16 == 2 ? 1u : 0u)) & 7u;
+					worst = std::max(worst, ++count[b]);
+				}
+			} else {
+				for(unsigned lane = 0; lane < group; ++lane) {
+					const unsigned b = w(insert_zeros(lane, g.st[s].rsorted, (int)RB)) & bank_mask;
+					worst = std::max(worst, ++count[b]);
+				}
 			}
 			total += worst;
 		}
