@@ -627,8 +627,30 @@ Cx overlay_remove(const tmfqs_register_view &v, Cx l) {
 	return cdiv(csub(l, {v.bias_re, v.bias_im}), {v.scale_re, v.scale_im});
 }
 
-// Exact logical amplitude sum (quantum_register.cpp:176-190).
+// Logical amplitude sum for the fast forms (complex64, or complex128 with
+// TMFQS_OPT_EXACT off): one FP64 read pass, the overlay applied as
+// scale * sum + N * bias.
+Cx fast_logical_sum(tmfqs_gpu_state *h, const tmfqs_register_view &v) {
+	const unsigned nb = tqb::sum_fast_blocks(ctx(h));
+	ensure_dev_small(h, nb * sizeof(double2));
+	if(h->pinned_elems < 2 * (size_t)nb) fail(TMFQS_ERR_LOGIC, "fast sum: pinned staging too small");
+	tqb::launch_sum_fast(ctx(h), h->precision, h->amps, h->N, static_cast<double2 *>(h->dev_small));
+	check_cuda(cudaMemcpyAsync(h->pinned, h->dev_small, nb * sizeof(double2), cudaMemcpyDeviceToHost, h->stream),
+	           "fast sum read");
+	check_cuda(cudaStreamSynchronize(h->stream), "fast sum sync");
+	Cx sum{0.0, 0.0};
+	for(unsigned b = 0; b < nb; ++b) {
+		sum.re += h->pinned[2 * b];
+		sum.im += h->pinned[2 * b + 1];
+	}
+	if(!v.overlay) return sum;
+	return cadd(cmul({v.scale_re, v.scale_im}, sum), cscale({v.bias_re, v.bias_im}, (double)h->N));
+}
+
+// Exact logical amplitude sum (quantum_register.cpp:176-190); the fast forms
+// take the one-pass FP64 sum.
 Cx logical_sum(tmfqs_gpu_state *h, const tmfqs_register_view &v) {
+	if(h->precision == TMFQS_FP32 || !h->opt_exact) return fast_logical_sum(h, v);
 	tqb::Overlay ov;
 	ov.active = v.overlay != 0;
 	ov.sre = v.scale_re;

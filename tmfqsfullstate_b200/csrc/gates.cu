@@ -139,6 +139,37 @@ __global__ void k_affine(typename Vec2<R>::type *a, uint64_t N, R sr, R si, R br
 	}
 }
 
+// The sum of all amplitudes in FP64 for the fast forms: each thread adds its
+// share in a fixed order, the warps and then the block add theirs, and the
+// caller adds the block partials in block order (deterministic; one read of
+// the state).  The exact forms use the sequential-sum engine instead.
+template <typename R>
+__global__ void __launch_bounds__(256) k_sum_fast(const typename Vec2<R>::type *a, uint64_t N, double2 *part) {
+	double sr = 0.0, si = 0.0;
+#pragma unroll 4
+	for(uint64_t i = gtid(); i < N; i += gstride()) {
+		const auto v = a[i];
+		sr += (double)v.x;
+		si += (double)v.y;
+	}
+#pragma unroll
+	for(int o = 16; o; o >>= 1) {
+		sr += __shfl_xor_sync(0xffffffffu, sr, o);
+		si += __shfl_xor_sync(0xffffffffu, si, o);
+	}
+	__shared__ double2 ws[8];
+	if((threadIdx.x & 31u) == 0) ws[threadIdx.x >> 5] = make_double2(sr, si);
+	__syncthreads();
+	if(threadIdx.x == 0) {
+		double2 t = make_double2(0.0, 0.0);
+		for(unsigned w = 0; w < (blockDim.x >> 5); ++w) {
+			t.x += ws[w].x;
+			t.y += ws[w].y;
+		}
+		part[blockIdx.x] = t;
+	}
+}
+
 template <typename R>
 __global__ void k_scatter_uniform(typename Vec2<R>::type *a, const uint64_t *states, uint64_t count, R amp) {
 	for(uint64_t i = gtid(); i < count; i += gstride()) {
@@ -372,6 +403,13 @@ void launch_affine(const LaunchCtx &c, int prec, void *a, unsigned n, double sre
 	const uint64_t N = 1ull << n;
 	TQB_DISPATCH(prec, k_affine<R><<<grid_for(c, N), kThreads, 0, c.stream>>>(static_cast<Vec2<R>::type *>(a), N, (R)sre, (R)sim, (R)bre, (R)bim));
 	after_launch(c, "affine");
+}
+
+unsigned sum_fast_blocks(const LaunchCtx &c) { return (unsigned)c.num_sms * 8u; }
+
+void launch_sum_fast(const LaunchCtx &c, int prec, const void *a, uint64_t N, double2 *part) {
+	TQB_DISPATCH(prec, k_sum_fast<R><<<sum_fast_blocks(c), 256, 0, c.stream>>>(static_cast<const Vec2<R>::type *>(a), N, part));
+	after_launch(c, "fast sum");
 }
 
 void launch_scatter_uniform(const LaunchCtx &c, int prec, void *a, const uint64_t *states, uint64_t count, double amp) {

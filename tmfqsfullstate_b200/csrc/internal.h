@@ -83,6 +83,10 @@ void launch_phase_flip(const LaunchCtx &c, int prec, void *a, uint64_t s);
 void launch_inversion(const LaunchCtx &c, int prec, void *a, unsigned n, double two_mre, double two_mim);
 void launch_affine(const LaunchCtx &c, int prec, void *a, unsigned n, double sre, double sim, double bre,
                    double bim);
+// Fast forms: the amplitude sum in FP64, one partial (re, im) per block of
+// sum_fast_blocks(c) blocks into `part`, added by the caller in block order.
+unsigned sum_fast_blocks(const LaunchCtx &c);
+void launch_sum_fast(const LaunchCtx &c, int prec, const void *a, uint64_t N, double2 *part);
 void launch_scatter_uniform(const LaunchCtx &c, int prec, void *a, const uint64_t *states, uint64_t count,
                             double amp);
 void launch_scatter_values(const LaunchCtx &c, int prec, void *a, const uint64_t *idx, const double *vals,
