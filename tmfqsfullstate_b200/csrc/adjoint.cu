@@ -13,8 +13,8 @@
 //       2 * sum_{x: both bits set} (Im(lambda_x) Re(psi_x) - Re(lambda_x) Im(psi_x))
 //   with lambda and psi taken at the end of the run (the phases of the later
 //   gates of the run cancel in conj(lambda_x) psi_x).
-// Per-block FP64 partial sums go to a buffer the host adds in block order, so
-// the results do not depend on scheduling.
+// Per-block FP64 partial sums stay on the device and are added in block order
+// (k_sum_partials), so the results do not depend on scheduling.
 #include <algorithm>
 #include <cmath>
 
@@ -184,6 +184,19 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 	}
 }
 
+// One block per partial-sum array, one thread per column.
+__global__ void k_sum_partials(const double *partials, size_t chunk_doubles, const __grid_constant__ PartialChunks t,
+                               double *out) {
+	const unsigned i = blockIdx.x, k = threadIdx.x;
+	const unsigned stride = t.stride[i];
+	double s = 0.0;
+	if(k < stride) {
+		const double *p = partials + (size_t)i * chunk_doubles + k;
+		for(unsigned b = 0; b < t.blocks[i]; ++b) s += p[(size_t)b * stride];
+	}
+	out[i * kMaxDiagRun + k] = s;
+}
+
 size_t grad_smem(size_t acc_bytes, unsigned nbytes) {
 	return acc_bytes * (kAdjThreads / 32) * kMaxDiagRun * 32 + sizeof(uint32_t) * 256 * nbytes;
 }
@@ -215,6 +228,18 @@ unsigned launch_obs_apply(const LaunchCtx &c, int prec, const void *psi, void *l
 	check_cuda(cudaGetLastError(), "observable");
 	if(c.launches) ++*c.launches;
 	return blocks;
+}
+
+void launch_sum_partials(const LaunchCtx &c, const double *partials, size_t chunk_doubles, const PartialChunks &t,
+                         double *out) {
+	if(t.count == 0) return;
+	if(t.count > kMaxPendingSums) fail(TMFQS_ERR_LOGIC, "adjoint: partial-sum table size");
+	for(unsigned i = 0; i < t.count; ++i)
+		if(t.stride[i] == 0 || t.stride[i] > kMaxDiagRun || (size_t)t.blocks[i] * t.stride[i] > chunk_doubles)
+			fail(TMFQS_ERR_LOGIC, "adjoint: partial-sum array shape");
+	k_sum_partials<<<t.count, kMaxDiagRun, 0, c.stream>>>(partials, chunk_doubles, t, out);
+	check_cuda(cudaGetLastError(), "partial sums");
+	if(c.launches) ++*c.launches;
 }
 
 unsigned launch_grad_run(const LaunchCtx &c, int prec, void *lam, void *psi, unsigned n, const DiagEntry *entries,

@@ -60,7 +60,7 @@ struct DeviceScope {
 };
 
 tqb::LaunchCtx ctx(tmfqs_gpu_state *h) {
-	return tqb::LaunchCtx{h->stream, h->num_sms, &h->stats.kernel_launches, h->err_dev};
+	return tqb::LaunchCtx{h->stream, h->num_sms, &h->stats.kernel_launches, h->err_dev, &h->ring};
 }
 
 // Reports (and clears) a failure recorded by a bounded device wait since the
@@ -956,7 +956,9 @@ size_t run_dense_block(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t i, size_t
 }
 
 // tmfqs_gpu_apply_ops: the Simulator's gate runs through the fusion planner.
-void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count) {
+// With sync false the passes are left in flight on the handle's stream (the
+// caller synchronises and checks the device error word).
+void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool sync = true) {
 	ensure_initialized(h, "operation batch");
 	if(count && !ops) fail(TMFQS_ERR_INVALID_ARGUMENT, "null op list");
 	DeviceScope d(h);
@@ -968,7 +970,10 @@ void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count) {
 			if(ops[i].kind == TMFQS_OP_GATE) run_gate(h, ops[i].matrix, ops[i].qubits, ops[i].k);
 			else p.run_single(ops[i]);
 		}
-		check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
+		if(sync) {
+			check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
+			check_device_error(h);
+		}
 		return;
 	}
 	Planner p(h);
@@ -1018,8 +1023,10 @@ void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count) {
 		p.flush();
 		throw;
 	}
-	check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
-	check_device_error(h);
+	if(sync) {
+		check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
+		check_device_error(h);
+	}
 }
 
 // ---- adjoint gradient (tmfqs_gpu_adjoint_gradient) ----
@@ -1053,17 +1060,77 @@ void free_adjoint_buffers(tmfqs_gpu_state *h) {
 
 bool is_diagonal_op(const tmfqs_op &op) { return op.kind == TMFQS_OP_CPHASE || op.kind == TMFQS_OP_PHASE_FLIP; }
 
-// Sum of per-block partials (block order), column k of a [blocks][stride] array.
-std::vector<double> read_partials(tmfqs_gpu_state *h, const double *dev, unsigned blocks, unsigned stride) {
-	std::vector<double> host((size_t)blocks * stride);
-	check_cuda(cudaMemcpyAsync(host.data(), dev, host.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
-	           "partials read");
-	check_cuda(cudaStreamSynchronize(h->stream), "partials sync");
-	std::vector<double> sum(stride, 0.0);
-	for(unsigned b = 0; b < blocks; ++b)
-		for(unsigned k = 0; k < stride; ++k) sum[k] += host[(size_t)b * stride + k];
-	return sum;
-}
+// The work handles of an adjoint call run on the caller's stream for the
+// duration of the call, so one stream orders every pass and no host waits
+// are needed between them; their own streams come back on exit.
+struct StreamBorrow {
+	tmfqs_gpu_state *owner;
+	tmfqs_gpu_state *w[2];
+	cudaStream_t saved[2];
+	StreamBorrow(tmfqs_gpu_state *h, tmfqs_gpu_state *a, tmfqs_gpu_state *b) : owner(h), w{a, b}, saved{a->stream, b->stream} {
+		a->stream = b->stream = h->stream;
+	}
+	~StreamBorrow() {
+		cudaStreamSynchronize(owner->stream);
+		w[0]->stream = saved[0];
+		w[1]->stream = saved[1];
+	}
+};
+
+// Gradient partial sums kept on the device: each launch writes its own array
+// of the handle's scratch, and one reduction and one read serve them all (or
+// every kMaxPendingSums arrays, when a circuit has more diagonal runs).
+class PendingSums {
+public:
+	struct Use {
+		size_t st, e;  // ops [st, e) of a diagonal run; st == e: the expectation
+	};
+	PendingSums(tmfqs_gpu_state *h, double *part, size_t chunk_doubles, double *out, const tmfqs_op *ops,
+	            const std::vector<size_t> &param_of, double *expectation, double *grads)
+	    : h_(h), part_(part), chunk_(chunk_doubles), out_(out), ops_(ops), param_of_(param_of), expectation_(expectation),
+	      grads_(grads) {
+		tab_.count = 0;
+	}
+	// Scratch for the next launch's partials (flushing first when full).
+	double *next() {
+		if(tab_.count == tqb::kMaxPendingSums) flush();
+		return part_ + (size_t)tab_.count * chunk_;
+	}
+	void add(unsigned blocks, unsigned stride, Use u) {
+		tab_.blocks[tab_.count] = blocks;
+		tab_.stride[tab_.count] = stride;
+		uses_.push_back(u);
+		++tab_.count;
+	}
+	void flush() {
+		if(!tab_.count) return;
+		tqb::launch_sum_partials(ctx(h_), part_, chunk_, tab_, out_);
+		std::vector<double> host((size_t)tab_.count * tqb::kMaxDiagRun);
+		check_cuda(cudaMemcpyAsync(host.data(), out_, host.size() * sizeof(double), cudaMemcpyDeviceToHost, h_->stream),
+		           "partials read");
+		check_cuda(cudaStreamSynchronize(h_->stream), "partials sync");
+		for(unsigned c = 0; c < tab_.count; ++c) {
+			const double *g = host.data() + (size_t)c * tqb::kMaxDiagRun;
+			const Use &u = uses_[c];
+			if(u.st == u.e) *expectation_ = g[0];
+			for(size_t k = u.st; k < u.e; ++k)
+				if(ops_[k].kind == TMFQS_OP_CPHASE) grads_[param_of_[k]] = 2.0 * g[k - u.st];
+		}
+		tab_.count = 0;
+		uses_.clear();
+	}
+
+private:
+	tmfqs_gpu_state *h_;
+	double *part_;
+	size_t chunk_;
+	double *out_;
+	const tmfqs_op *ops_;
+	const std::vector<size_t> &param_of_;
+	double *expectation_, *grads_;
+	tqb::PartialChunks tab_;
+	std::vector<Use> uses_;
+};
 
 void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, const uint64_t *masks,
                       const double *weights, unsigned terms, size_t every, double *expectation, double *grads) {
@@ -1105,32 +1172,39 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 		}
 		h->adj_ckpt_bytes = nseg * bytes;
 	}
+	// Scratch: kMaxPendingSums partial arrays of the largest launch, then the
+	// reduced sums.
+	const size_t chunk = (size_t)tqb::adjoint_max_blocks(h->num_sms) * tqb::kMaxDiagRun;
 	if(!h->adj_part &&
-	   cudaMalloc(&h->adj_part, (size_t)tqb::adjoint_max_blocks(h->num_sms) * tqb::kMaxDiagRun * sizeof(double)) != cudaSuccess) {
+	   cudaMalloc(&h->adj_part, (chunk * tqb::kMaxPendingSums + tqb::kMaxPendingSums * tqb::kMaxDiagRun) * sizeof(double)) !=
+	       cudaSuccess) {
 		cudaGetLastError();
 		h->adj_part = nullptr;
 		fail(TMFQS_ERR_NOMEM, "adjoint gradient: scratch allocation failed");
 	}
 	unsigned char *ckb = static_cast<unsigned char *>(h->adj_ckpt);
-	double *partials = static_cast<double *>(h->adj_part);
-
-	// Forward pass, with psi saved after every segment of K ops.
-	for(size_t sidx = 0; sidx < nseg; ++sidx) {
-		const size_t a0 = sidx * K, len = std::min(K, count - a0);
-		apply_ops_body(h, ops + a0, len);
-		check_cuda(cudaMemcpyAsync(ckb + sidx * bytes, h->amps, bytes, cudaMemcpyDeviceToDevice, h->stream), "checkpoint");
-	}
-	check_cuda(cudaStreamSynchronize(h->stream), "forward sync");
+	double *part = static_cast<double *>(h->adj_part);
+	PendingSums sums(h, part, chunk, part + chunk * tqb::kMaxPendingSums, ops, param_of, expectation, grads);
 
 	struct {
 		tmfqs_gpu_state *h;
 	} lam{work_handle(h, h->adj_lam)}, psi{work_handle(h, h->adj_psi)};
-	unsigned blocks;
+	StreamBorrow borrow(h, lam.h, psi.h);
+
+	// Forward pass, with psi saved after every segment of K ops.
+	for(size_t sidx = 0; sidx < nseg; ++sidx) {
+		const size_t a0 = sidx * K, len = std::min(K, count - a0);
+		apply_ops_body(h, ops + a0, len, false);
+		check_cuda(cudaMemcpyAsync(ckb + sidx * bytes, h->amps, bytes, cudaMemcpyDeviceToDevice, h->stream), "checkpoint");
+	}
+
 	{
 		PassTimer timer(h, TMFQS_KT_ADJOINT, sweep_bytes(h));
-		blocks = tqb::launch_obs_apply(ctx(h), h->precision, h->amps, lam.h->amps, h->n, masks, weights, terms, partials);
+		double *dst = sums.next();
+		const unsigned blocks =
+		    tqb::launch_obs_apply(ctx(h), h->precision, h->amps, lam.h->amps, h->n, masks, weights, terms, dst);
+		sums.add(blocks, 1, {0, 0});
 	}
-	*expectation = read_partials(h, partials, blocks, 1)[0];
 
 	// Backward pass: segment by segment, psi restored from its checkpoint.
 	for(size_t sidx = nseg; sidx-- > 0;) {
@@ -1139,8 +1213,6 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 		std::vector<char> cp_before(b0 - a0 + 1, 0);
 		for(size_t i = a0; i < b0; ++i) cp_before[i - a0 + 1] = cp_before[i - a0] || ops[i].kind == TMFQS_OP_CPHASE;
 		check_cuda(cudaMemcpyAsync(psi.h->amps, ckb + sidx * bytes, bytes, cudaMemcpyDeviceToDevice, h->stream), "restore");
-		// psi's own passes run on its stream.
-		check_cuda(cudaStreamSynchronize(h->stream), "restore sync");
 		size_t i = b0;
 		while(i > a0) {
 			const bool diag = is_diagonal_op(ops[i - 1]);
@@ -1161,12 +1233,11 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 					const bool need_psi = cp_before[st - a0] != 0;
 					{
 						PassTimer timer(h, TMFQS_KT_ADJOINT, sweep_bytes(h) * (need_psi ? 2.0 : 1.5));
-						blocks = tqb::launch_grad_run(ctx(h), h->precision, lam.h->amps, psi.h->amps, h->n, ent.data(),
-						                              (unsigned)ent.size(), need_psi, partials);
+						double *dst = sums.next();
+						const unsigned blocks = tqb::launch_grad_run(ctx(h), h->precision, lam.h->amps, psi.h->amps, h->n,
+						                                             ent.data(), (unsigned)ent.size(), need_psi, dst);
+						sums.add(blocks, tqb::kMaxDiagRun, {st, e});
 					}
-					const std::vector<double> g = read_partials(h, partials, blocks, tqb::kMaxDiagRun);
-					for(size_t k = st; k < e; ++k)
-						if(ops[k].kind == TMFQS_OP_CPHASE) grads[param_of[k]] = 2.0 * g[k - st];
 					e = st;
 				}
 			} else {
@@ -1188,13 +1259,17 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 					}
 					inv.push_back(op);
 				}
-				apply_ops_body(lam.h, inv.data(), inv.size());
-				if(cp_before[j - a0]) apply_ops_body(psi.h, inv.data(), inv.size());
+				apply_ops_body(lam.h, inv.data(), inv.size(), false);
+				if(cp_before[j - a0]) apply_ops_body(psi.h, inv.data(), inv.size(), false);
 			}
 			i = j;
 		}
 	}
+	sums.flush();
 	check_cuda(cudaStreamSynchronize(h->stream), "backward sync");
+	check_device_error(h);
+	check_device_error(lam.h);
+	check_device_error(psi.h);
 }
 
 // ===========================================================================
@@ -1232,7 +1307,16 @@ int tmfqs_gpu_create(int precision, int device, tmfqs_gpu_state **out) {
 				fail(TMFQS_ERR_NOMEM, "pinned error word allocation failed");
 			}
 			*h->err_host = 0;
+			if(cudaMallocHost(&h->ring.host, tqb::UploadRing::kSlots * tqb::UploadRing::kSlotBytes) != cudaSuccess) {
+				cudaGetLastError();
+				h->ring.host = nullptr;  // uploads fall back to synchronous copies
+			}
+			for(unsigned k = 0; k < tqb::UploadRing::kSlots; ++k)
+				check_cuda(cudaEventCreateWithFlags(&h->ring.ev[k], cudaEventDisableTiming), "upload event");
 		} catch(...) {
+			for(unsigned k = 0; k < tqb::UploadRing::kSlots; ++k)
+				if(h->ring.ev[k]) cudaEventDestroy(h->ring.ev[k]);
+			if(h->ring.host) cudaFreeHost(h->ring.host);
 			if(h->err_host) cudaFreeHost(h->err_host);
 			if(h->pinned) cudaFreeHost(h->pinned);
 			if(h->stream) cudaStreamDestroy(h->stream);
@@ -1260,6 +1344,9 @@ int tmfqs_gpu_destroy(tmfqs_gpu_state *h) {
 		if(h->dev_prog) cudaFree(h->dev_prog);
 		if(h->pinned) cudaFreeHost(h->pinned);
 		if(h->err_host) cudaFreeHost(h->err_host);
+		for(unsigned k = 0; k < tqb::UploadRing::kSlots; ++k)
+			if(h->ring.ev[k]) cudaEventDestroy(h->ring.ev[k]);
+		if(h->ring.host) cudaFreeHost(h->ring.host);
 		if(h->stream) cudaStreamDestroy(h->stream);
 		delete h;
 	});

@@ -609,12 +609,11 @@ void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 		}
 		dev_prog_bytes = need * 2;
 	}
-	// The program buffer is reused: make sure the previous pass consumed it.
+	// The program buffer is reused: the upload is ordered on the stream after the pass that read it last.
 	std::vector<unsigned char> host(need, 0);
 	std::memcpy(host.data(), pass.ops.data(), ops_bytes);
 	if(!pass.chain.empty()) std::memcpy(host.data() + ph_off, pass.chain.data(), pass.chain.size() * sizeof(ChainEntry));
-	check_cuda(cudaMemcpyAsync(dev_prog, host.data(), need, cudaMemcpyHostToDevice, c.stream), "fused program upload");
-	check_cuda(cudaStreamSynchronize(c.stream), "fused program upload sync");
+	upload_async(c, dev_prog, host.data(), need, "fused program upload");
 	const size_t smem = (sizeof(typename Vec2<R>::type) << pass.K) + (sizeof(uint64_t) << (pass.K - g.m));
 	check_cuda(cudaFuncSetAttribute(k_fused<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fused smem");
 	int per_sm = 1;

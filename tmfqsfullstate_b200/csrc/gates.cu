@@ -7,6 +7,8 @@
 #include <cmath>
 #include <vector>
 
+#include <cstring>
+
 #include "device_common.cuh"
 #include "internal.h"
 
@@ -27,6 +29,27 @@ void after_launch(const LaunchCtx &c, const char *what) {
 	check_cuda(cudaGetLastError(), what);
 	if(c.launches) ++*c.launches;
 }
+
+}  // namespace
+
+void upload_async(const LaunchCtx &c, void *dev, const void *src, size_t bytes, const char *what) {
+	UploadRing *r = c.ring;
+	if(!r || !r->host || bytes > UploadRing::kSlotBytes) {
+		check_cuda(cudaMemcpyAsync(dev, src, bytes, cudaMemcpyHostToDevice, c.stream), what);
+		check_cuda(cudaStreamSynchronize(c.stream), what);
+		return;
+	}
+	const unsigned s = r->next;
+	r->next = (s + 1) % UploadRing::kSlots;
+	if(r->pending[s]) check_cuda(cudaEventSynchronize(r->ev[s]), what);
+	unsigned char *slot = r->host + (size_t)s * UploadRing::kSlotBytes;
+	std::memcpy(slot, src, bytes);
+	check_cuda(cudaMemcpyAsync(dev, slot, bytes, cudaMemcpyHostToDevice, c.stream), what);
+	check_cuda(cudaEventRecord(r->ev[s], c.stream), what);
+	r->pending[s] = true;
+}
+
+namespace {
 
 // applyHadamard, dense_state_backend.cpp:255-274: pairs (s0, s0|m), skip
 // all-zero pairs, a0' = (a0+a1)*inv, a1' = (a0-a1)*inv per component.

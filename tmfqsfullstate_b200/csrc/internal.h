@@ -66,12 +66,29 @@ SeqResult seq_sample_static(int precision, const void *amps, unsigned num_qubits
 // ---------------------------------------------------------------------------
 // Single-operation kernels (gates.cu)
 // ---------------------------------------------------------------------------
+// Pinned staging slots for small host-to-device uploads (pass programs): a
+// copy leaves the host at once and a slot is reused only after its copy has
+// completed, so the host can plan passes while the GPU runs earlier ones.
+struct UploadRing {
+	static constexpr unsigned kSlots = 8;
+	static constexpr size_t kSlotBytes = size_t(64) << 10;
+	unsigned char *host = nullptr;
+	cudaEvent_t ev[kSlots] = {};
+	bool pending[kSlots] = {};
+	unsigned next = 0;
+};
+
 struct LaunchCtx {
 	cudaStream_t stream;
 	int num_sms;
 	uint64_t *launches;
-	int *err = nullptr;  // device-visible error word of the handle (nonzero: a bounded wait gave up)
+	int *err = nullptr;          // device-visible error word of the handle (nonzero: a bounded wait gave up)
+	UploadRing *ring = nullptr;  // the handle's upload slots
 };
+
+// Copies `bytes` from host memory to `dev` in stream order: through a slot of
+// the context's ring when it fits (no host wait), else synchronously.
+void upload_async(const LaunchCtx &c, void *dev, const void *src, size_t bytes, const char *what);
 
 void launch_h(const LaunchCtx &c, int prec, void *a, unsigned n, unsigned bit);
 void launch_x(const LaunchCtx &c, int prec, void *a, unsigned n, unsigned bit);
@@ -184,6 +201,20 @@ unsigned launch_obs_apply(const LaunchCtx &c, int prec, const void *psi, void *l
 unsigned launch_grad_run(const LaunchCtx &c, int prec, void *lam, void *psi, unsigned n, const DiagEntry *entries,
                          unsigned count, bool uncompute_psi, double *dev_partials);
 
+// Partial-sum arrays left on the device by the launches above, reduced
+// together: array i starts at partials + i * chunk_doubles and holds
+// blocks[i] rows of stride[i] (<= kMaxDiagRun) columns.
+constexpr unsigned kMaxPendingSums = 64;
+struct PartialChunks {
+	unsigned count;
+	unsigned blocks[kMaxPendingSums];
+	unsigned stride[kMaxPendingSums];
+};
+// out[i * kMaxDiagRun + k] = sum of column k of array i over its rows, added
+// in row order in FP64 (the order a host loop over the blocks uses).
+void launch_sum_partials(const LaunchCtx &c, const double *partials, size_t chunk_doubles, const PartialChunks &t,
+                         double *out);
+
 // ---------------------------------------------------------------------------
 // Tensor-core dense gates on complex64 states (tc_gate.cu)
 // ---------------------------------------------------------------------------
@@ -264,6 +295,7 @@ struct tmfqs_gpu_state {
 	bool opt_qft_pass = true;  // fast forms: QFT ladder segments on the dedicated QFT pass
 	int *err_host = nullptr;   // mapped pinned error word written by bounded device waits
 	int *err_dev = nullptr;
+	tqb::UploadRing ring;      // pinned staging for pass programs
 	void *dev_tc = nullptr; // tensor-core gate operands
 	size_t dev_tc_bytes = 0;
 	// Adjoint-gradient work buffers, kept for the next call (freed by destroy):

@@ -779,8 +779,7 @@ bool run_radix(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	std::memcpy(host.data() + o_tb, P.tabs.data(), P.tabs.size() * sizeof(double2));
 	std::memcpy(host.data() + o_sl, P.slots.data(), P.slots.size() * sizeof(RadixSlot));
 	std::memcpy(host.data() + o_tm, P.terms.data(), P.terms.size() * sizeof(RadixTerm));
-	check_cuda(cudaMemcpyAsync(dev_prog, host.data(), upload, cudaMemcpyHostToDevice, c.stream), "radix program upload");
-	check_cuda(cudaStreamSynchronize(c.stream), "radix program upload sync");
+	upload_async(c, dev_prog, host.data(), upload, "radix program upload");
 	unsigned char *pbase = static_cast<unsigned char *>(dev_prog);
 	V *otab = reinterpret_cast<V *>(pbase + o_ot);
 	if(P.g.nslots) {
