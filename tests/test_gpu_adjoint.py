@@ -180,6 +180,48 @@ def test_adjoint_general_circuit_matches_fd():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n,prec,tol", [(2, tq.FP64, 1e-8), (2, tq.FP32, 1e-5), (3, tq.FP64, 1e-8),
+                                        (12, tq.FP64, 1e-8), (12, tq.FP32, 1e-5)])
+def test_adjoint_long_diagonal_runs(n, prec, tol):
+    """Diagonal runs of 40, 12 and 20 gates (gradient passes of 32, 8, 12 and 20
+    entries: one to four phase tables), phase flips inside the runs, masks on
+    the low three bits and above them, and registers of fewer than eight
+    amplitudes."""
+    rng = np.random.default_rng(17 + n)
+    masks, weights = [0b1, (1 << n) - 1, 0b11 << (n - 2)], [0.6, -1.1, 0.9]
+    o = diag_values(n, masks, weights)
+    skeleton = [(0, [q], 0) for q in range(n)]
+    for run_len in (40, 12, 20):
+        for _ in range(run_len):
+            q = [int(v) for v in rng.permutation(n)[:2]]
+            skeleton.append((3 if rng.random() < 0.75 else 5, q, int(rng.integers(0, 1 << n))))
+        skeleton += [(0, [int(rng.integers(0, n))], 0), (1, [int(rng.integers(0, n))], 0)]
+    count = sum(1 for k, _, _ in skeleton if k == 3)
+    th = rng.uniform(-np.pi, np.pi, count)
+
+    def build(thetas, oracle):
+        out, it = [], iter(thetas)
+        lib = O if oracle else tq
+        for kind, q, s in skeleton:
+            if kind == 0:
+                out.append(lib.h(q[0]))
+            elif kind == 1:
+                out.append(lib.x(q[0]))
+            elif kind == 3:
+                out.append(lib.cphase(q[0], q[1], float(next(it))))
+            else:
+                out.append(lib.phase_flip(s))
+        return out
+
+    with tq.GpuState(prec) as g:
+        g.init_basis(n, 0)
+        e, grads = g.adjoint_gradient(build(th, False), masks, weights, 0)
+    assert abs(e - energy(n, build(th, True), o)) < tol
+    fd = fd_grad(n, lambda t: build(t, True), th, o)
+    assert np.max(np.abs(grads - fd)) < tol
+
+
+@pytest.mark.gpu
 def test_adjoint_torch_autograd():
     import torch
 

@@ -27,7 +27,7 @@ namespace {
 
 constexpr unsigned kAdjThreads = 256;
 constexpr unsigned kBatch = 4;      // amplitudes per thread per loop trip (observable)
-constexpr unsigned kGradBatch = 4;  // the same for the gradient runs
+constexpr unsigned kGradBatch = 8;  // consecutive amplitudes per thread per loop trip (gradient runs)
 
 struct ObsParams {
 	uint64_t mask[kMaxObsTerms];
@@ -85,23 +85,33 @@ __global__ void __launch_bounds__(kAdjThreads) k_obs_apply(const typename Vec2<R
 	if(threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
-// Conjugate of a unit phase times v.
-template <typename V, typename R>
-__device__ __forceinline__ V mul_conj(V v, R c, R s) {
-	V r;
-	r.x = fma(c, v.x, s * v.y);
-	r.y = fma(c, v.y, -(s * v.x));
-	return r;
-}
-
 // Which entries of a run act on basis state x: an entry's condition (x
 // contains its mask, or x equals the flipped state) holds exactly when it
 // holds byte by byte, so the set of entries hitting x is the AND of one
-// 32-bit table word per index byte.  Each lane accumulates its terms in its own
-// shared-memory column (entry-major, no bank conflicts), touching only the
-// entries that hit.  A: FP32 columns for complex64 (a lane adds a few hundred
-// terms, far inside the form's tolerance), FP64 for complex128; block and grid
-// sums are FP64.
+// 32-bit table word per index byte ("hit" word, bit k for entry k).
+//
+// The inverse of the run multiplies amplitude x by the product of the
+// conjugate phases of its hit entries (-1 for a flip).  The gates commute, so
+// the product is taken byte by byte over the hit word: four tables of 256
+// products (formed in FP64, rounded once to the storage type) and at most
+// three complex products per amplitude.
+//
+// Gradients: a thread owns kGradBatch = 8 consecutive amplitudes x0 + u, so
+// for a controlled phase with mask m the condition splits into its low part
+// c = m & 7 (on u) and the rest (on x0, the same for all eight).  Every
+// entry whose rest holds (the hit word of x0 | 7, flips removed) receives the
+// superset sum S[c] = sum over u containing c of v(x0 + u), once per batch.
+// Each lane adds these into its own shared-memory column (entry-major, no
+// bank conflicts).  A: FP32 columns for complex64, FP64 for complex128; block
+// and grid sums are FP64.
+template <typename V, typename R>
+__device__ __forceinline__ V cmul(V a, V b) {
+	V r;
+	r.x = fma(a.x, b.x, -(a.y * b.y));
+	r.y = fma(a.x, b.y, a.y * b.x);
+	return r;
+}
+
 template <typename R, typename A>
 __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::type *lam, typename Vec2<R>::type *psi,
                                                             uint64_t N, RunParams rp, unsigned nbytes, int uncompute_psi,
@@ -109,16 +119,36 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 	typedef typename Vec2<R>::type V;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	A *accs = reinterpret_cast<A *>(smem_raw);                                              // [warps][entries][32]
-	uint32_t *tab = reinterpret_cast<uint32_t *>(accs + (kAdjThreads / 32) * kMaxDiagRun * 32);  // [nbytes][256]
+	V *qtab = reinterpret_cast<V *>(accs + (kAdjThreads / 32) * kMaxDiagRun * 32);           // [4][256]
+	uint32_t *tab = reinterpret_cast<uint32_t *>(qtab + 4 * 256);                           // [nbytes][256]
 	__shared__ double red[kAdjThreads / 32];
-	__shared__ R scr[kMaxDiagRun], sci[kMaxDiagRun];
+	__shared__ uint32_t cls[kGradBatch];
 	const unsigned count = rp.count;
+	const unsigned nq = (count + 7) / 8;  // phase tables in use
 	uint32_t flips = 0;
 	for(unsigned k = 0; k < count; ++k)
 		if(rp.kind[k] == kDiagFlip) flips |= 1u << k;
-	for(unsigned k = threadIdx.x; k < kMaxDiagRun; k += blockDim.x) {
-		scr[k] = k < count ? (R)rp.cr[k] : R(1);
-		sci[k] = k < count ? (R)rp.ci[k] : R(0);
+	if(threadIdx.x < kGradBatch) {
+		uint32_t m = 0;
+		for(unsigned k = 0; k < count; ++k)
+			if(!((flips >> k) & 1u) && (unsigned)(rp.mask[k] & (kGradBatch - 1)) == threadIdx.x) m |= 1u << k;
+		cls[threadIdx.x] = m;
+	}
+	for(unsigned e = threadIdx.x; e < nq * 256; e += blockDim.x) {
+		const unsigned j = e >> 8, v = e & 255u;
+		double pr = 1.0, pi = 0.0;
+		for(unsigned b = 0; b < 8; ++b) {
+			const unsigned k = 8 * j + b;
+			if(k >= count || !((v >> b) & 1u)) continue;
+			const double c = ((flips >> k) & 1u) ? -1.0 : rp.cr[k], sn = ((flips >> k) & 1u) ? 0.0 : -rp.ci[k];
+			const double tr = pr * c - pi * sn;
+			pi = pr * sn + pi * c;
+			pr = tr;
+		}
+		V q;
+		q.x = (R)pr;
+		q.y = (R)pi;
+		qtab[e] = q;
 	}
 	for(unsigned e = threadIdx.x; e < nbytes * 256; e += blockDim.x) {
 		const unsigned j = e >> 8, v = e & 255u;
@@ -135,41 +165,50 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 	const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
 	A *col = accs + warp * kMaxDiagRun * 32 + lane;
 	const uint32_t all = count >= 32 ? ~0u : ((1u << count) - 1u);
+	uint32_t cm[kGradBatch];
+#pragma unroll
+	for(unsigned c = 0; c < kGradBatch; ++c) cm[c] = cls[c];
+	// A register of fewer than kGradBatch amplitudes (n < 3) fills the batch
+	// with zero terms.
+	const unsigned lim = N < kGradBatch ? (unsigned)N : kGradBatch;
 	for(uint64_t x0 = gtid() * kGradBatch; x0 < N; x0 += gstride() * kGradBatch) {
 		V lb[kGradBatch], pb[kGradBatch];
 #pragma unroll
 		for(unsigned u = 0; u < kGradBatch; ++u)
-			if(x0 + u < N) {
+			if(u < lim) {
 				lb[u] = lam[x0 + u];
 				pb[u] = psi[x0 + u];
 			}
+		uint32_t hh = all;
+		for(unsigned j = 1; j < nbytes; ++j) hh &= tab[(j << 8) | ((unsigned)(x0 >> (8 * j)) & 255u)];
+		const unsigned b0 = (unsigned)x0 & 255u;
+		A S[kGradBatch];
 #pragma unroll
 		for(unsigned u = 0; u < kGradBatch; ++u) {
-			const uint64_t x = x0 + u;
-			if(x >= N) break;
-			uint32_t hit = all;
-			for(unsigned j = 0; j < nbytes; ++j) hit &= tab[(j << 8) | ((unsigned)(x >> (8 * j)) & 255u)];
-			if(!hit) continue;
+			S[u] = A(0);
+			if(u >= lim) continue;
 			V l = lb[u], p = pb[u];
-			const A v = (A)l.y * (A)p.x - (A)l.x * (A)p.y;
-			for(uint32_t c = hit & ~flips; c; c &= c - 1u) col[(__ffs(c) - 1) * 32] += v;
-			// The run's inverse, last gate first.
-			for(uint32_t c = hit; c;) {
-				const int k = 31 - __clz(c);
-				c ^= 1u << k;
-				if((flips >> k) & 1u) {
-					l.x = -l.x;
-					l.y = -l.y;
-					p.x = -p.x;
-					p.y = -p.y;
-				} else {
-					const R cr = scr[k], ci = sci[k];
-					l = mul_conj(l, cr, ci);
-					if(uncompute_psi) p = mul_conj(p, cr, ci);
-				}
-			}
-			lam[x] = l;
-			if(uncompute_psi) psi[x] = p;
+			S[u] = (A)l.y * (A)p.x - (A)l.x * (A)p.y;
+			// Table entry 0 is the empty product 1, which leaves a value unchanged.
+			const uint32_t hit = hh & tab[b0 | u];
+			V P = qtab[hit & 255u];
+			if(nq > 1) P = cmul<V, R>(P, qtab[256 | ((hit >> 8) & 255u)]);
+			if(nq > 2) P = cmul<V, R>(P, qtab[512 | ((hit >> 16) & 255u)]);
+			if(nq > 3) P = cmul<V, R>(P, qtab[768 | (hit >> 24)]);
+			lam[x0 + u] = cmul<V, R>(l, P);
+			if(uncompute_psi) psi[x0 + u] = cmul<V, R>(p, P);
+		}
+		// Superset sums over the three low bits.
+#pragma unroll
+		for(unsigned b = 0; b < 3; ++b)
+#pragma unroll
+			for(unsigned u = 0; u < kGradBatch; ++u)
+				if(!((u >> b) & 1u)) S[u] += S[u | (1u << b)];
+		const uint32_t rest = hh & tab[b0 | (kGradBatch - 1)] & ~flips;
+		if(rest) {
+#pragma unroll
+			for(unsigned c = 0; c < kGradBatch; ++c)
+				for(uint32_t m = rest & cm[c]; m; m &= m - 1u) col[(__ffs(m) - 1) * 32] += S[c];
 		}
 	}
 	__syncthreads();
@@ -197,8 +236,8 @@ __global__ void k_sum_partials(const double *partials, size_t chunk_doubles, con
 	out[i * kMaxDiagRun + k] = s;
 }
 
-size_t grad_smem(size_t acc_bytes, unsigned nbytes) {
-	return acc_bytes * (kAdjThreads / 32) * kMaxDiagRun * 32 + sizeof(uint32_t) * 256 * nbytes;
+size_t grad_smem(size_t acc_bytes, size_t vec_bytes, unsigned nbytes) {
+	return acc_bytes * (kAdjThreads / 32) * kMaxDiagRun * 32 + vec_bytes * 4 * 256 + sizeof(uint32_t) * 256 * nbytes;
 }
 
 unsigned adj_blocks(const LaunchCtx &c, uint64_t N) {
@@ -258,12 +297,12 @@ unsigned launch_grad_run(const LaunchCtx &c, int prec, void *lam, void *psi, uns
 	const int up = uncompute_psi ? 1 : 0;
 	const unsigned nbytes = (n + 7) / 8;
 	if(prec == TMFQS_FP64) {
-		const size_t smem = grad_smem(sizeof(double), nbytes);
+		const size_t smem = grad_smem(sizeof(double), sizeof(double2), nbytes);
 		check_cuda(cudaFuncSetAttribute(k_grad_run<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "gradient smem");
 		k_grad_run<double, double><<<blocks, kAdjThreads, smem, c.stream>>>(static_cast<double2 *>(lam), static_cast<double2 *>(psi), N, rp,
 		                                                                    nbytes, up, dev_partials);
 	} else {
-		const size_t smem = grad_smem(sizeof(float), nbytes);
+		const size_t smem = grad_smem(sizeof(float), sizeof(float2), nbytes);
 		check_cuda(cudaFuncSetAttribute(k_grad_run<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "gradient smem");
 		k_grad_run<float, float><<<blocks, kAdjThreads, smem, c.stream>>>(static_cast<float2 *>(lam), static_cast<float2 *>(psi), N, rp,
 		                                                                  nbytes, up, dev_partials);
