@@ -310,18 +310,18 @@ struct Planner {
 	explicit Planner(tmfqs_gpu_state *hh) : h(hh) {
 		// Tiles of 2^12 complex128 / 2^13 complex64 amplitudes (64 KB).  The
 		// exact form keeps rows of >= 128 bytes local; the fast forms' radix
-		// passes copy 16-byte granules and take 64-byte rows, which leaves one
-		// more bit per pass for the circuit.
+		// passes copy 16-byte granules and take rows of 32 (complex128) or 64
+		// (complex64) bytes, which leaves more bits per pass for the circuit.
 		const unsigned Kmax = h->precision == TMFQS_FP64 ? 12u : 13u;
 		const bool fast = !h->opt_exact || h->precision == TMFQS_FP32;
 		if(fast && h->opt_radix) {
-			// Rows of 64 bytes at least; wider rows (up to 256 bytes) stream far
-			// better when the other local bits are high, so take the widest
-			// that still covers all n bits in the fewest passes.
-			const unsigned mmin = h->precision == TMFQS_FP64 ? 2u : 3u, mmax = mmin + 2u;
+			// Wider rows (up to four times the narrowest) stream far better when
+			// the other local bits are high, so take the widest that still
+			// covers all n bits in the fewest passes.
 			auto passes = [&](unsigned m) -> unsigned {
 				return h->n <= Kmax ? 1u : 1u + (h->n - Kmax + (Kmax - m) - 1u) / (Kmax - m);
 			};
+			const unsigned mmin = h->precision == TMFQS_FP64 ? 2u : 3u, mmax = mmin + 2u;
 			mlow = mmin;
 			for(unsigned m = mmin + 1; m <= mmax; ++m)
 				if(passes(m) == passes(mmin)) mlow = m;
@@ -1031,8 +1031,9 @@ void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool 
 
 // ---- adjoint gradient (tmfqs_gpu_adjoint_gradient) ----
 // A work handle of `h` (kept in *w between calls) with h's options and a state
-// of h->n qubits.
-tmfqs_gpu_state *work_handle(tmfqs_gpu_state *h, tmfqs_gpu_state *&w) {
+// of h->n qubits; without a state buffer of its own when `with_state` is false
+// (the caller points it at one).
+tmfqs_gpu_state *work_handle(tmfqs_gpu_state *h, tmfqs_gpu_state *&w, bool with_state = true) {
 	if(!w) {
 		const int rc = tmfqs_gpu_create(h->precision, h->device, &w);
 		if(rc) throw tqb::Error{rc, g_last_error};
@@ -1042,7 +1043,19 @@ tmfqs_gpu_state *work_handle(tmfqs_gpu_state *h, tmfqs_gpu_state *&w) {
 	w->opt_exact = h->opt_exact;
 	w->opt_radix = h->opt_radix;
 	w->opt_qft_pass = h->opt_qft_pass;
-	ensure_state(w, h->n);
+	if(with_state) {
+		ensure_state(w, h->n);
+	} else {
+		if(w->amps) {
+			check_cuda(cudaStreamSynchronize(w->stream), "sync before free");
+			cudaFree(w->amps);
+			w->amps = nullptr;
+		}
+		tqb::seq_scratch_free(w->seq);
+		w->bytes = amp_bytes(w) << h->n;
+		w->n = h->n;
+		w->N = 1ull << h->n;
+	}
 	w->initialized = true;
 	return w;
 }
@@ -1062,18 +1075,23 @@ bool is_diagonal_op(const tmfqs_op &op) { return op.kind == TMFQS_OP_CPHASE || o
 
 // The work handles of an adjoint call run on the caller's stream for the
 // duration of the call, so one stream orders every pass and no host waits
-// are needed between them; their own streams come back on exit.
+// are needed between them.  Their own streams and state buffers (psi works
+// in place on the checkpoints) come back on exit.
 struct StreamBorrow {
 	tmfqs_gpu_state *owner;
 	tmfqs_gpu_state *w[2];
 	cudaStream_t saved[2];
-	StreamBorrow(tmfqs_gpu_state *h, tmfqs_gpu_state *a, tmfqs_gpu_state *b) : owner(h), w{a, b}, saved{a->stream, b->stream} {
+	void *amps[2];
+	StreamBorrow(tmfqs_gpu_state *h, tmfqs_gpu_state *a, tmfqs_gpu_state *b)
+	    : owner(h), w{a, b}, saved{a->stream, b->stream}, amps{a->amps, b->amps} {
 		a->stream = b->stream = h->stream;
 	}
 	~StreamBorrow() {
 		cudaStreamSynchronize(owner->stream);
-		w[0]->stream = saved[0];
-		w[1]->stream = saved[1];
+		for(int i = 0; i < 2; ++i) {
+			w[i]->stream = saved[i];
+			w[i]->amps = amps[i];
+		}
 	}
 };
 
@@ -1188,7 +1206,7 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 
 	struct {
 		tmfqs_gpu_state *h;
-	} lam{work_handle(h, h->adj_lam)}, psi{work_handle(h, h->adj_psi)};
+	} lam{work_handle(h, h->adj_lam)}, psi{work_handle(h, h->adj_psi, false)};
 	StreamBorrow borrow(h, lam.h, psi.h);
 
 	// Forward pass, with psi saved after every segment of K ops.
@@ -1212,7 +1230,9 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 		// cp_before[i - a0]: a controlled phase lies in [a0, i).
 		std::vector<char> cp_before(b0 - a0 + 1, 0);
 		for(size_t i = a0; i < b0; ++i) cp_before[i - a0 + 1] = cp_before[i - a0] || ops[i].kind == TMFQS_OP_CPHASE;
-		check_cuda(cudaMemcpyAsync(psi.h->amps, ckb + sidx * bytes, bytes, cudaMemcpyDeviceToDevice, h->stream), "restore");
+		// psi = the state after the segment: its checkpoint, used in place (each
+		// checkpoint is read by one segment only).
+		psi.h->amps = ckb + sidx * bytes;
 		size_t i = b0;
 		while(i > a0) {
 			const bool diag = is_diagonal_op(ops[i - 1]);
