@@ -52,7 +52,9 @@ constexpr unsigned kRadixMaxSlots = 48;
 //                   Hadamards in bit order, and after the one on bit i the
 //                   controlled phases pi/2^(j-i) with every later bit j, as a
 //                   compiled butterfly network with the roots of unity below
-enum RadixItemKind : uint32_t { kRIButterfly = 0, kRIButterflyTw = 1, kRIDiag = 2, kRIQft = 3 };
+//   kRIWalsh        butterflies on register bits 0..d-1 (d in bits 8-15), no
+//                   phases between them: one compiled network
+enum RadixItemKind : uint32_t { kRIButterfly = 0, kRIButterflyTw = 1, kRIDiag = 2, kRIQft = 3, kRIWalsh = 4 };
 
 struct RadixStage {
 	uint32_t first, count;    // items of the stage
@@ -178,6 +180,27 @@ __device__ __forceinline__ void rbfly_dispatch(V (&v)[1 << RB], unsigned b, cons
 	}
 }
 
+template <typename V, int RB, int D>
+__device__ __forceinline__ void walsh_stage(V (&v)[1 << RB]) {
+	if constexpr(D > 0) rbfly<V, RB, 0>(v, nullptr);
+	if constexpr(D > 1) rbfly<V, RB, 1>(v, nullptr);
+	if constexpr(D > 2) rbfly<V, RB, 2>(v, nullptr);
+	if constexpr(D > 3) rbfly<V, RB, 3>(v, nullptr);
+	if constexpr(D > 4) rbfly<V, RB, 4>(v, nullptr);
+}
+
+template <typename V, int RB>
+__device__ __forceinline__ void walsh_dispatch(V (&v)[1 << RB], unsigned d) {
+	switch(d) {
+		case 1: walsh_stage<V, RB, 1>(v); break;
+		case 2: if constexpr(RB >= 2) walsh_stage<V, RB, 2>(v); break;
+		case 3: if constexpr(RB >= 3) walsh_stage<V, RB, 3>(v); break;
+		case 4: if constexpr(RB >= 4) walsh_stage<V, RB, 4>(v); break;
+		case 5: if constexpr(RB >= 5) walsh_stage<V, RB, 5>(v); break;
+		default: break;
+	}
+}
+
 template <typename V, int RB>
 __device__ __forceinline__ void qft_dispatch(V (&v)[1 << RB], unsigned d, const RadixGeom &g) {
 	switch(d) {
@@ -247,6 +270,25 @@ __device__ __forceinline__ void apply_factors(V (&v)[1 << RB], const RadixSmem<V
 	}
 #pragma unroll
 	for(int r = 1; r < (1 << RB); ++r) v[r] = vmul(v[r], F[r]);
+}
+
+// The constant factor alone (mask 1, no per-thread terms): one value for every
+// register, and a real product when it has no imaginary part (the scale of a
+// pass without phases on its non-register bits).
+template <typename V, int RB>
+__device__ __forceinline__ void apply_constant(V (&v)[1 << RB], const RadixSmem<V> &sh, const V *ot, unsigned s,
+                                               unsigned ia, unsigned ib, unsigned lo, unsigned nb) {
+	const V f = vmul(vmul(sh.A[(s << lo) + ia], sh.B[s * nb + ib]), ot[s]);
+	if(f.y == 0) {
+#pragma unroll
+		for(int r = 0; r < (1 << RB); ++r) {
+			v[r].x *= f.x;
+			v[r].y *= f.x;
+		}
+	} else {
+#pragma unroll
+		for(int r = 0; r < (1 << RB); ++r) v[r] = vmul(v[r], f);
+	}
 }
 
 }  // namespace
@@ -378,7 +420,9 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 				const uint32_t it = sh.items[k];
 				const unsigned kind = it & 0xffu, b = (it >> 8) & 0xffu;
 				const V *tb = sh.tabs + (it >> 16);
-				if(kind == kRIQft) {
+				if(kind == kRIWalsh) {
+					walsh_dispatch<V, RB>(v, b);
+				} else if(kind == kRIQft) {
 					qft_dispatch<V, RB>(v, b, g);
 				} else if(kind == kRIDiag) {
 #pragma unroll
@@ -387,7 +431,9 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 					rbfly_dispatch<V, RB>(v, b, kind == kRIButterflyTw ? tb : nullptr);
 				}
 			}
-			if(S.post_mask)
+			if(S.post_mask == 1u && !S.post_xcount)
+				apply_constant<V, RB>(v, sh, ot, S.post_slot, ia, ib, g.lo, nb);
+			else if(S.post_mask)
 				apply_factors<V, RB>(v, sh, ot, S.post_slot, S.post_mask, ia, ib, g.lo, nb, gterms, S.post_xfirst, S.post_xcount, jt,
 				                     cbase);
 			const bool last = st + 1 == g.nstages;
@@ -648,7 +694,28 @@ bool build_radix_program(const FusedPass &pass, unsigned K, size_t vbytes, Radix
 				seen |= 1u << other;
 			}
 		}
-		if(qft) {
+		// Hadamards on register bits 0..d-1 with no phase between them (they
+		// commute): one compiled network, then the in-stage phases that follow
+		// the last of them.  When that one is on bit d-1 and has phases, it
+		// stays a butterfly item of its own (its phases then ride on its |1>
+		// outputs).
+		bool walsh = d > 1 && !qft && (int)seq.size() == d;
+		uint32_t wseen = 0;
+		for(int i = 0; walsh && i < d; ++i) {
+			const int r = seq[i].first;
+			if(r < 0 || r >= d || ((wseen >> r) & 1u) || (i + 1 < d && !seq[i].second.empty())) walsh = false;
+			else wseen |= 1u << r;
+		}
+		const bool tail_own = walsh && !seq.back().second.empty() && seq.back().first == d - 1;
+		if(walsh && (!tail_own || d >= 3)) {
+			P.items.push_back(kRIWalsh | ((uint32_t)(tail_own ? d - 1 : d) << 8));
+			if(tail_own) {
+				P.items.push_back(kRIButterfly | ((uint32_t)(d - 1) << 8));
+				last_bfly = d - 1;
+			}
+			run = seq.back().second;
+			flush_run();
+		} else if(qft) {
 			P.items.push_back(kRIQft | ((uint32_t)d << 8));
 		} else {
 			for(auto &e : seq) {
