@@ -150,6 +150,8 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 		q.y = (R)pi;
 		qtab[e] = q;
 	}
+	// Byte 0 is stored transposed, [v & 7][v >> 3]: a warp's lanes look up
+	// b0 | u with b0 = 8 * lane, on 32 consecutive words.
 	for(unsigned e = threadIdx.x; e < nbytes * 256; e += blockDim.x) {
 		const unsigned j = e >> 8, v = e & 255u;
 		uint32_t bits = 0;
@@ -158,7 +160,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 			const bool ok = ((flips >> k) & 1u) ? v == mb : (v & mb) == mb;
 			bits |= (ok ? 1u : 0u) << k;
 		}
-		tab[e] = bits;
+		tab[j ? e : (((v & 7u) << 5) | (v >> 3))] = bits;
 	}
 	for(unsigned e = threadIdx.x; e < (kAdjThreads / 32) * kMaxDiagRun * 32; e += blockDim.x) accs[e] = A(0);
 	__syncthreads();
@@ -173,16 +175,32 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 	const unsigned lim = N < kGradBatch ? (unsigned)N : kGradBatch;
 	for(uint64_t x0 = gtid() * kGradBatch; x0 < N; x0 += gstride() * kGradBatch) {
 		V lb[kGradBatch], pb[kGradBatch];
+		if constexpr(sizeof(V) == 8) {
+			if(lim == kGradBatch) {
+				// Eight complex64 values: four 16-byte loads each (x0 is a multiple of 8).
+				const float4 *l4 = reinterpret_cast<const float4 *>(lam + x0), *p4 = reinterpret_cast<const float4 *>(psi + x0);
+#pragma unroll
+				for(unsigned q = 0; q < kGradBatch / 2; ++q) {
+					const float4 a = l4[q], b = p4[q];
+					lb[2 * q] = V{a.x, a.y};
+					lb[2 * q + 1] = V{a.z, a.w};
+					pb[2 * q] = V{b.x, b.y};
+					pb[2 * q + 1] = V{b.z, b.w};
+				}
+			}
+		}
 #pragma unroll
 		for(unsigned u = 0; u < kGradBatch; ++u)
-			if(u < lim) {
+			if(u < lim && (sizeof(V) != 8 || lim < kGradBatch)) {
 				lb[u] = lam[x0 + u];
 				pb[u] = psi[x0 + u];
 			}
 		uint32_t hh = all;
 		for(unsigned j = 1; j < nbytes; ++j) hh &= tab[(j << 8) | ((unsigned)(x0 >> (8 * j)) & 255u)];
-		const unsigned b0 = (unsigned)x0 & 255u;
+		const unsigned b0s = ((unsigned)x0 & 255u) >> 3;  // byte 0 of x0, transposed index
 		A S[kGradBatch];
+		// complex64: the results wait in registers for 16-byte stores.
+		V lo[sizeof(V) == 8 ? kGradBatch : 1], po[sizeof(V) == 8 ? kGradBatch : 1];
 #pragma unroll
 		for(unsigned u = 0; u < kGradBatch; ++u) {
 			S[u] = A(0);
@@ -190,13 +208,28 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 			V l = lb[u], p = pb[u];
 			S[u] = (A)l.y * (A)p.x - (A)l.x * (A)p.y;
 			// Table entry 0 is the empty product 1, which leaves a value unchanged.
-			const uint32_t hit = hh & tab[b0 | u];
+			const uint32_t hit = hh & tab[(u << 5) | b0s];
 			V P = qtab[hit & 255u];
 			if(nq > 1) P = cmul<V, R>(P, qtab[256 | ((hit >> 8) & 255u)]);
 			if(nq > 2) P = cmul<V, R>(P, qtab[512 | ((hit >> 16) & 255u)]);
 			if(nq > 3) P = cmul<V, R>(P, qtab[768 | (hit >> 24)]);
-			lam[x0 + u] = cmul<V, R>(l, P);
-			if(uncompute_psi) psi[x0 + u] = cmul<V, R>(p, P);
+			if(sizeof(V) == 8 && lim == kGradBatch) {
+				lo[sizeof(V) == 8 ? u : 0] = cmul<V, R>(l, P);
+				po[sizeof(V) == 8 ? u : 0] = cmul<V, R>(p, P);
+			} else {
+				lam[x0 + u] = cmul<V, R>(l, P);
+				if(uncompute_psi) psi[x0 + u] = cmul<V, R>(p, P);
+			}
+		}
+		if constexpr(sizeof(V) == 8) {
+			if(lim == kGradBatch) {
+				float4 *l4 = reinterpret_cast<float4 *>(lam + x0), *p4 = reinterpret_cast<float4 *>(psi + x0);
+#pragma unroll
+				for(unsigned q = 0; q < kGradBatch / 2; ++q) {
+					l4[q] = make_float4(lo[2 * q].x, lo[2 * q].y, lo[2 * q + 1].x, lo[2 * q + 1].y);
+					if(uncompute_psi) p4[q] = make_float4(po[2 * q].x, po[2 * q].y, po[2 * q + 1].x, po[2 * q + 1].y);
+				}
+			}
 		}
 		// Superset sums over the three low bits.
 #pragma unroll
@@ -204,11 +237,25 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 #pragma unroll
 			for(unsigned u = 0; u < kGradBatch; ++u)
 				if(!((u >> b) & 1u)) S[u] += S[u | (1u << b)];
-		const uint32_t rest = hh & tab[b0 | (kGradBatch - 1)] & ~flips;
+		const uint32_t rest = hh & tab[((kGradBatch - 1) << 5) | b0s] & ~flips;
 		if(rest) {
+			// Columns of distinct entries never alias: the next column is read
+			// before the current one is written, so the reads overlap.
 #pragma unroll
-			for(unsigned c = 0; c < kGradBatch; ++c)
-				for(uint32_t m = rest & cm[c]; m; m &= m - 1u) col[(__ffs(m) - 1) * 32] += S[c];
+			for(unsigned c = 0; c < kGradBatch; ++c) {
+				uint32_t m = rest & cm[c];
+				if(!m) continue;
+				A *p = col + (__ffs(m) - 1) * 32;
+				A cur = *p;
+				for(m &= m - 1u; m; m &= m - 1u) {
+					A *q = col + (__ffs(m) - 1) * 32;
+					const A nxt = *q;
+					*p = cur + S[c];
+					p = q;
+					cur = nxt;
+				}
+				*p = cur + S[c];
+			}
 		}
 	}
 	__syncthreads();
