@@ -13,8 +13,8 @@
 //       2 * sum_{x: both bits set} (Im(lambda_x) Re(psi_x) - Re(lambda_x) Im(psi_x))
 //   with lambda and psi taken at the end of the run (the phases of the later
 //   gates of the run cancel in conj(lambda_x) psi_x).
-// Per-block FP64 partial sums stay on the device and are added in block order
-// (k_sum_partials), so the results do not depend on scheduling.
+// Per-block FP64 partial sums stay on the device and are added in a fixed
+// order (k_sum_partials), so the results do not depend on scheduling.
 #include <algorithm>
 #include <cmath>
 
@@ -55,11 +55,32 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 	return s;
 }
 
+// O(x) = sum_j w_j (-1)^parity(x & m_j).  The parities of all terms form one
+// 64-bit word, the XOR over the index bytes of x of a per-byte table word
+// (bit j: parity of that byte of x & m_j); O(x) is then the sum over the
+// word's bytes of a table of signed weight sums (256 per byte of terms, FP64).
 template <typename R>
 __global__ void __launch_bounds__(kAdjThreads) k_obs_apply(const typename Vec2<R>::type *psi, typename Vec2<R>::type *lam,
-                                                          uint64_t N, ObsParams p, double *partials) {
+                                                          uint64_t N, ObsParams p, unsigned nbytes, double *partials) {
 	typedef typename Vec2<R>::type V;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	uint64_t *par = reinterpret_cast<uint64_t *>(smem_raw);     // [nbytes][256]; byte 0 as [v & 3][v >> 2]
+	double *wsum = reinterpret_cast<double *>(par + nbytes * 256);  // [ceil(nterms / 8)][256]
 	__shared__ double red[kAdjThreads / 32];
+	const unsigned nt = (p.nterms + 7) / 8;
+	for(unsigned e = threadIdx.x; e < nbytes * 256; e += blockDim.x) {
+		const unsigned j = e >> 8, v = e & 255u;
+		uint64_t w = 0;
+		for(unsigned t = 0; t < p.nterms; ++t) w |= (uint64_t)(__popc(v & ((unsigned)(p.mask[t] >> (8 * j)) & 255u)) & 1) << t;
+		par[j ? e : (((v & 3u) << 6) | (v >> 2))] = w;
+	}
+	for(unsigned e = threadIdx.x; e < nt * 256; e += blockDim.x) {
+		const unsigned k = e >> 8, v = e & 255u;
+		double o = 0.0;
+		for(unsigned b = 0; b < 8 && 8 * k + b < p.nterms; ++b) o += ((v >> b) & 1u) ? -p.weight[8 * k + b] : p.weight[8 * k + b];
+		wsum[e] = o;
+	}
+	__syncthreads();
 	double acc = 0.0;
 	// kBatch consecutive amplitudes per thread, loads issued together.
 	for(uint64_t x0 = gtid() * kBatch; x0 < N; x0 += gstride() * kBatch) {
@@ -67,12 +88,16 @@ __global__ void __launch_bounds__(kAdjThreads) k_obs_apply(const typename Vec2<R
 #pragma unroll
 		for(unsigned u = 0; u < kBatch; ++u)
 			if(x0 + u < N) v[u] = psi[x0 + u];
+		uint64_t hi = 0;
+		for(unsigned j = 1; j < nbytes; ++j) hi ^= par[(j << 8) | ((unsigned)(x0 >> (8 * j)) & 255u)];
+		const unsigned b0s = ((unsigned)x0 & 255u) >> 2;
 #pragma unroll
 		for(unsigned u = 0; u < kBatch; ++u) {
 			const uint64_t x = x0 + u;
 			if(x >= N) break;
-			double o = 0.0;
-			for(unsigned j = 0; j < p.nterms; ++j) o += (__popcll(x & p.mask[j]) & 1) ? -p.weight[j] : p.weight[j];
+			const uint64_t w = hi ^ par[(u << 6) | b0s];
+			double o = wsum[w & 255u];
+			for(unsigned k = 1; k < nt; ++k) o += wsum[(k << 8) | ((unsigned)(w >> (8 * k)) & 255u)];
 			const double re = (double)v[u].x, im = (double)v[u].y;
 			acc += o * (re * re + im * im);
 			V l;
@@ -270,17 +295,20 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 	}
 }
 
-// One block per partial-sum array, one thread per column.
+// One block per partial-sum array, one warp per column: lane l adds rows
+// l, l + 32, ... in row order, then the warp adds its lanes in a fixed tree.
 __global__ void k_sum_partials(const double *partials, size_t chunk_doubles, const __grid_constant__ PartialChunks t,
                                double *out) {
-	const unsigned i = blockIdx.x, k = threadIdx.x;
+	const unsigned i = blockIdx.x, k = threadIdx.y, lane = threadIdx.x;
 	const unsigned stride = t.stride[i];
 	double s = 0.0;
 	if(k < stride) {
 		const double *p = partials + (size_t)i * chunk_doubles + k;
-		for(unsigned b = 0; b < t.blocks[i]; ++b) s += p[(size_t)b * stride];
+		for(unsigned b = lane; b < t.blocks[i]; b += 32) s += p[(size_t)b * stride];
 	}
-	out[i * kMaxDiagRun + k] = s;
+#pragma unroll
+	for(int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+	if(lane == 0) out[i * kMaxDiagRun + k] = s;
 }
 
 size_t grad_smem(size_t acc_bytes, size_t vec_bytes, unsigned nbytes) {
@@ -307,10 +335,17 @@ unsigned launch_obs_apply(const LaunchCtx &c, int prec, const void *psi, void *l
 	p.nterms = nterms;
 	const uint64_t N = 1ull << n;
 	const unsigned blocks = adj_blocks(c, N);
-	if(prec == TMFQS_FP64)
-		k_obs_apply<double><<<blocks, kAdjThreads, 0, c.stream>>>(static_cast<const double2 *>(psi), static_cast<double2 *>(lam), N, p, dev_partials);
-	else
-		k_obs_apply<float><<<blocks, kAdjThreads, 0, c.stream>>>(static_cast<const float2 *>(psi), static_cast<float2 *>(lam), N, p, dev_partials);
+	const unsigned nbytes = (n + 7) / 8;
+	const size_t smem = sizeof(uint64_t) * 256 * nbytes + sizeof(double) * 256 * ((nterms + 7) / 8);
+	if(prec == TMFQS_FP64) {
+		check_cuda(cudaFuncSetAttribute(k_obs_apply<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "observable smem");
+		k_obs_apply<double><<<blocks, kAdjThreads, smem, c.stream>>>(static_cast<const double2 *>(psi), static_cast<double2 *>(lam), N, p,
+		                                                              nbytes, dev_partials);
+	} else {
+		check_cuda(cudaFuncSetAttribute(k_obs_apply<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "observable smem");
+		k_obs_apply<float><<<blocks, kAdjThreads, smem, c.stream>>>(static_cast<const float2 *>(psi), static_cast<float2 *>(lam), N, p,
+		                                                             nbytes, dev_partials);
+	}
 	check_cuda(cudaGetLastError(), "observable");
 	if(c.launches) ++*c.launches;
 	return blocks;
@@ -323,7 +358,7 @@ void launch_sum_partials(const LaunchCtx &c, const double *partials, size_t chun
 	for(unsigned i = 0; i < t.count; ++i)
 		if(t.stride[i] == 0 || t.stride[i] > kMaxDiagRun || (size_t)t.blocks[i] * t.stride[i] > chunk_doubles)
 			fail(TMFQS_ERR_LOGIC, "adjoint: partial-sum array shape");
-	k_sum_partials<<<t.count, kMaxDiagRun, 0, c.stream>>>(partials, chunk_doubles, t, out);
+	k_sum_partials<<<t.count, dim3(32, kMaxDiagRun), 0, c.stream>>>(partials, chunk_doubles, t, out);
 	check_cuda(cudaGetLastError(), "partial sums");
 	if(c.launches) ++*c.launches;
 }

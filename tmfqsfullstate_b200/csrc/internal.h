@@ -210,8 +210,9 @@ struct PartialChunks {
 	unsigned blocks[kMaxPendingSums];
 	unsigned stride[kMaxPendingSums];
 };
-// out[i * kMaxDiagRun + k] = sum of column k of array i over its rows, added
-// in row order in FP64 (the order a host loop over the blocks uses).
+// out[i * kMaxDiagRun + k] = sum of column k of array i over its rows, in FP64
+// and in a fixed order (32 interleaved row-order sums, then a fixed tree), so
+// the result does not depend on scheduling.
 void launch_sum_partials(const LaunchCtx &c, const double *partials, size_t chunk_doubles, const PartialChunks &t,
                          double *out);
 

@@ -92,6 +92,7 @@ struct RadixGeom {
 	unsigned lpos[14];          // ascending local bit positions
 	uint64_t ntiles;
 	unsigned nstages, nitems, ntab, nslots, nterms;
+	unsigned outer_free;        // no slot has outer terms: every tile's outer row is the slot scales
 	RootTable roots;            // twiddles of the compiled QFT stages
 };
 
@@ -352,8 +353,9 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 				const unsigned j = q * per16;
 				cp_async16(dst + rswz<V>(j), a + (base | scatter(j)));
 			}
-			for(unsigned q = tid; q < ot_stride / per16; q += nthr)
-				cp_async16(odst + q * per16, otab + o * ot_stride + q * per16);
+			if(!g.outer_free)
+				for(unsigned q = tid; q < ot_stride / per16; q += nthr)
+					cp_async16(odst + q * per16, otab + o * ot_stride + q * per16);
 		}
 		cp_async_commit();
 	};
@@ -364,6 +366,14 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 	for(unsigned k = tid; k < g.nstages; k += nthr) sh.stages[k] = gstages[k];
 	for(unsigned k = tid; k < g.nitems; k += nthr) sh.items[k] = gitems[k];
 	for(unsigned k = tid; k < g.ntab; k += nthr) sh.tabs[k] = to_v<V>(gtabs[k]);
+	// Without outer terms the outer rows of both buffers hold the slot scales
+	// for every tile (cos 0 and sin 0 times the scale, as the table would).
+	if(g.outer_free)
+		for(unsigned s = tid; s < g.nslots; s += nthr) {
+			const V w = to_v<V>(make_double2(gslots[s].scale, 0.0));
+			sh.Ot[0][s] = w;
+			sh.Ot[1][s] = w;
+		}
 	// Tile-independent phase tables of the local control bits, in FP64.
 	const unsigned na = 1u << g.lo;
 	for(unsigned t = tid; t < g.nslots * (na + nb); t += nthr) {
@@ -790,6 +800,9 @@ bool build_radix_program(const FusedPass &pass, unsigned K, size_t vbytes, Radix
 	g.ntab = (unsigned)P.tabs.size();
 	g.nslots = (unsigned)P.slots.size();
 	g.nterms = (unsigned)P.terms.size();
+	g.outer_free = 1;
+	for(const RadixSlot &sl : P.slots)
+		if(sl.o_count) g.outer_free = 0;
 	return g.nitems <= kRadixMaxItems && g.ntab <= kRadixMaxTab && g.nslots <= kRadixMaxSlots;
 }
 
@@ -849,7 +862,7 @@ bool run_radix(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	upload_async(c, dev_prog, host.data(), upload, "radix program upload");
 	unsigned char *pbase = static_cast<unsigned char *>(dev_prog);
 	V *otab = reinterpret_cast<V *>(pbase + o_ot);
-	if(P.g.nslots) {
+	if(P.g.nslots && !P.g.outer_free) {
 		const uint64_t work = P.g.ntiles * P.g.nslots;
 		const unsigned blocks = (unsigned)std::min<uint64_t>((work + 255) / 256, (uint64_t)c.num_sms * 8);
 		k_outer_table<R><<<blocks, 256, 0, c.stream>>>(otab, ot_stride, P.g, reinterpret_cast<const RadixSlot *>(pbase + o_sl),
