@@ -60,6 +60,9 @@ struct RadixStage {
 	uint32_t first, count;    // items of the stage
 	uint32_t rbit[5];         // register bit i -> local bit
 	uint32_t rsorted[5];      // the register local bits, ascending
+	uint32_t imask[5];        // (1 << rsorted[i]) - 1: the thread index gets a zero bit inserted above it
+	uint32_t roff[5];         // swizzled shared-memory offset of register bit i
+	uint64_t gbit[5];         // global index bit of register bit i (direct stores)
 	uint32_t pre_slot, pre_mask;    // first factor slot; bit 0 constant factor, bit i+1 register bit i
 	uint32_t post_slot, post_mask;
 	uint32_t direct;                // last stage: store to HBM from registers
@@ -118,14 +121,6 @@ template <>
 __device__ __forceinline__ unsigned rswz<float2>(unsigned j) {
 	// Keeps element pairs (16-byte copy granules) together.
 	return j ^ (((j >> 4) & 7u) << 1);
-}
-
-
-
-
-__device__ __forceinline__ unsigned rinsert0(unsigned x, unsigned b) {
-	const unsigned lo = x & ((1u << b) - 1u);
-	return ((x ^ lo) << 1) | lo;
 }
 
 // Angle of a slot's outer terms for the tile with base index `base`.
@@ -410,10 +405,10 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 			const RadixStage &S = sh.stages[st];
 			unsigned jt = tid;
 #pragma unroll
-			for(int i = 0; i < RB; ++i) jt = rinsert0(jt, S.rsorted[i]);
+			for(int i = 0; i < RB; ++i) jt = ((jt & ~S.imask[i]) << 1) | (jt & S.imask[i]);
 			unsigned roff[RB];
 #pragma unroll
-			for(int i = 0; i < RB; ++i) roff[i] = rswz<V>(1u << S.rbit[i]);
+			for(int i = 0; i < RB; ++i) roff[i] = S.roff[i];
 			const unsigned sj = rswz<V>(jt);
 			auto addr = [&](int r) -> unsigned {
 				unsigned x = sj;
@@ -452,7 +447,7 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 				const uint64_t gt = cbase | scatter(jt);
 				uint64_t gbit[RB];
 #pragma unroll
-				for(int i = 0; i < RB; ++i) gbit[i] = scatter(1u << S.rbit[i]);
+				for(int i = 0; i < RB; ++i) gbit[i] = S.gbit[i];
 #pragma unroll
 				for(int r = 0; r < (1 << RB); ++r) {
 					uint64_t x = gt;
@@ -616,6 +611,14 @@ bool build_radix_program(const FusedPass &pass, unsigned K, size_t vbytes, Radix
 		std::vector<unsigned> sorted(rb.begin(), rb.end());
 		std::sort(sorted.begin(), sorted.end());
 		for(int i = 0; i < RB; ++i) S.rsorted[i] = sorted[i];
+		for(int i = 0; i < RB; ++i) {
+			S.imask[i] = (1u << sorted[i]) - 1u;
+			const unsigned j = 1u << rb[i];
+			// rswz of the kernel: 16-byte values j ^ ((j >> 3) & 7), 8-byte values
+			// j ^ (((j >> 4) & 7) << 1).
+			S.roff[i] = vbytes == 16 ? (j ^ ((j >> 3) & 7u)) : (j ^ (((j >> 4) & 7u) << 1));
+			S.gbit[i] = 1ull << pass.lpos[rb[i]];
+		}
 		auto regidx = [&](const BitRef &r) -> int {
 			if(!r.local) return -1;
 			for(int i = 0; i < RB; ++i)
