@@ -106,6 +106,24 @@ def test_adjoint_layered_matches_fd(prec, exact, tol):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [(tq.FP64, 1e-8), (tq.FP32, 1e-4)])
+def test_adjoint_more_runs_than_pending_sums(prec, tol):
+    """70 diagonal runs: the device-side partial sums are read back mid-call
+    (every 64 passes) as well as at the end.  Complex64 over 910 ops: E drifts
+    by about 1e-5 (|O| <= 6), hence 1e-4."""
+    n, layers = 6, 70
+    th = tq.random_angles(n * layers, 77)
+    masks, weights = tq.zz_ring_observable(n)
+    o = diag_values(n, masks, weights)
+    with tq.GpuState(prec) as g:
+        g.init_basis(n, 0)
+        e, grads = g.adjoint_gradient(tq.layered_cphase_ops(n, th), masks, weights, 0)
+    assert abs(e - energy(n, layered_oracle(n)(th), o)) < tol
+    fd = fd_grad(n, layered_oracle(n), th, o)
+    assert np.max(np.abs(grads - fd)) < tol
+
+
+@pytest.mark.gpu
 def test_adjoint_checkpoint_intervals_agree():
     n, layers = 10, 4
     th = tq.random_angles(n * layers, 5)

@@ -40,6 +40,7 @@ struct RunParams {
 	double cr[kMaxDiagRun], ci[kMaxDiagRun];
 	int kind[kMaxDiagRun];       // DiagEntry kind
 	unsigned count;
+	unsigned nvary;              // leading entries that depend on index bits 0-2 (flips included)
 };
 
 __device__ __forceinline__ double block_sum(double v, double *red) {
@@ -198,6 +199,9 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 	// A register of fewer than kGradBatch amplitudes (n < 3) fills the batch
 	// with zero terms.
 	const unsigned lim = N < kGradBatch ? (unsigned)N : kGradBatch;
+	// The entries that depend on the three lowest index bits come first and
+	// number at most 8: bytes 1-3 of the hit word are the same for the batch.
+	const bool split = nq > 1 && rp.nvary <= 8;
 	for(uint64_t x0 = gtid() * kGradBatch; x0 < N; x0 += gstride() * kGradBatch) {
 		V lb[kGradBatch], pb[kGradBatch];
 		if constexpr(sizeof(V) == 8) {
@@ -223,6 +227,15 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 		uint32_t hh = all;
 		for(unsigned j = 1; j < nbytes; ++j) hh &= tab[(j << 8) | ((unsigned)(x0 >> (8 * j)) & 255u)];
 		const unsigned b0s = ((unsigned)x0 & 255u) >> 3;  // byte 0 of x0, transposed index
+		// Entries 8 and up hit all eight amplitudes alike (split runs): their
+		// phase product once per batch.
+		V Prest;
+		if(split) {
+			const uint32_t h7 = hh & tab[((kGradBatch - 1) << 5) | b0s];
+			Prest = qtab[256 | ((h7 >> 8) & 255u)];
+			if(nq > 2) Prest = cmul<V, R>(Prest, qtab[512 | ((h7 >> 16) & 255u)]);
+			if(nq > 3) Prest = cmul<V, R>(Prest, qtab[768 | (h7 >> 24)]);
+		}
 		A S[kGradBatch];
 		// complex64: the results wait in registers for 16-byte stores.
 		V lo[sizeof(V) == 8 ? kGradBatch : 1], po[sizeof(V) == 8 ? kGradBatch : 1];
@@ -235,9 +248,13 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 			// Table entry 0 is the empty product 1, which leaves a value unchanged.
 			const uint32_t hit = hh & tab[(u << 5) | b0s];
 			V P = qtab[hit & 255u];
-			if(nq > 1) P = cmul<V, R>(P, qtab[256 | ((hit >> 8) & 255u)]);
-			if(nq > 2) P = cmul<V, R>(P, qtab[512 | ((hit >> 16) & 255u)]);
-			if(nq > 3) P = cmul<V, R>(P, qtab[768 | (hit >> 24)]);
+			if(split) {
+				P = cmul<V, R>(P, Prest);
+			} else {
+				if(nq > 1) P = cmul<V, R>(P, qtab[256 | ((hit >> 8) & 255u)]);
+				if(nq > 2) P = cmul<V, R>(P, qtab[512 | ((hit >> 16) & 255u)]);
+				if(nq > 3) P = cmul<V, R>(P, qtab[768 | (hit >> 24)]);
+			}
 			if(sizeof(V) == 8 && lim == kGradBatch) {
 				lo[sizeof(V) == 8 ? u : 0] = cmul<V, R>(l, P);
 				po[sizeof(V) == 8 ? u : 0] = cmul<V, R>(p, P);
@@ -374,6 +391,11 @@ unsigned launch_grad_run(const LaunchCtx &c, int prec, void *lam, void *psi, uns
 		rp.kind[k] = entries[k].kind;
 	}
 	rp.count = count;
+	// The caller orders the entries that depend on bits 0-2 first; count them.
+	rp.nvary = 0;
+	while(rp.nvary < count && (entries[rp.nvary].kind == kDiagFlip || (entries[rp.nvary].mask & 7u))) ++rp.nvary;
+	for(unsigned k = rp.nvary; k < count; ++k)
+		if(entries[k].kind == kDiagFlip || (entries[k].mask & 7u)) rp.nvary = count;  // not ordered: no split
 	const uint64_t N = 1ull << n;
 	const unsigned blocks = adj_blocks(c, N);
 	const int up = uncompute_psi ? 1 : 0;

@@ -1101,7 +1101,8 @@ struct StreamBorrow {
 class PendingSums {
 public:
 	struct Use {
-		size_t st, e;  // ops [st, e) of a diagonal run; st == e: the expectation
+		bool obs;                    // the expectation (column 0)
+		std::vector<size_t> col_op;  // gradient pass: the op of each column
 	};
 	PendingSums(tmfqs_gpu_state *h, double *part, size_t chunk_doubles, double *out, const tmfqs_op *ops,
 	            const std::vector<size_t> &param_of, double *expectation, double *grads)
@@ -1117,7 +1118,7 @@ public:
 	void add(unsigned blocks, unsigned stride, Use u) {
 		tab_.blocks[tab_.count] = blocks;
 		tab_.stride[tab_.count] = stride;
-		uses_.push_back(u);
+		uses_.push_back(std::move(u));
 		++tab_.count;
 	}
 	void flush() {
@@ -1130,9 +1131,11 @@ public:
 		for(unsigned c = 0; c < tab_.count; ++c) {
 			const double *g = host.data() + (size_t)c * tqb::kMaxDiagRun;
 			const Use &u = uses_[c];
-			if(u.st == u.e) *expectation_ = g[0];
-			for(size_t k = u.st; k < u.e; ++k)
-				if(ops_[k].kind == TMFQS_OP_CPHASE) grads_[param_of_[k]] = 2.0 * g[k - u.st];
+			if(u.obs) *expectation_ = g[0];
+			for(size_t col = 0; col < u.col_op.size(); ++col) {
+				const size_t k = u.col_op[col];
+				if(ops_[k].kind == TMFQS_OP_CPHASE) grads_[param_of_[k]] = 2.0 * g[col];
+			}
 		}
 		tab_.count = 0;
 		uses_.clear();
@@ -1221,7 +1224,7 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 		double *dst = sums.next();
 		const unsigned blocks =
 		    tqb::launch_obs_apply(ctx(h), h->precision, h->amps, lam.h->amps, h->n, masks, weights, terms, dst);
-		sums.add(blocks, 1, {0, 0});
+		sums.add(blocks, 1, {true, {}});
 	}
 
 	// Backward pass: segment by segment, psi restored from its checkpoint.
@@ -1241,22 +1244,31 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 			if(diag) {
 				for(size_t e = i; e > j;) {
 					const size_t st = std::max(j, e > tqb::kMaxDiagRun ? e - tqb::kMaxDiagRun : 0);
+					// Entries that depend on the three lowest index bits (flips, and
+					// phases with a mask bit there) first: the gradient pass then
+					// looks up one phase table per amplitude when they fit in 8.
 					std::vector<tqb::DiagEntry> ent;
-					for(size_t k = st; k < e; ++k) {
-						const tmfqs_op &op = ops[k];
-						if(op.kind == TMFQS_OP_CPHASE)
-							ent.push_back({tqb::kDiagCPhase, (1ull << bit_of(h, op.q0)) | (1ull << bit_of(h, op.q1)),
-							               std::cos(op.theta), std::sin(op.theta)});
-						else
-							ent.push_back({tqb::kDiagFlip, op.state, 1.0, 0.0});
-					}
+					std::vector<size_t> col_op;
+					for(int low = 1; low >= 0; --low)
+						for(size_t k = st; k < e; ++k) {
+							const tmfqs_op &op = ops[k];
+							tqb::DiagEntry d;
+							if(op.kind == TMFQS_OP_CPHASE)
+								d = {tqb::kDiagCPhase, (1ull << bit_of(h, op.q0)) | (1ull << bit_of(h, op.q1)), std::cos(op.theta),
+								     std::sin(op.theta)};
+							else
+								d = {tqb::kDiagFlip, op.state, 1.0, 0.0};
+							if((d.kind == tqb::kDiagFlip || (d.mask & 7u)) != (low == 1)) continue;
+							ent.push_back(d);
+							col_op.push_back(k);
+						}
 					const bool need_psi = cp_before[st - a0] != 0;
 					{
 						PassTimer timer(h, TMFQS_KT_ADJOINT, sweep_bytes(h) * (need_psi ? 2.0 : 1.5));
 						double *dst = sums.next();
 						const unsigned blocks = tqb::launch_grad_run(ctx(h), h->precision, lam.h->amps, psi.h->amps, h->n,
 						                                             ent.data(), (unsigned)ent.size(), need_psi, dst);
-						sums.add(blocks, tqb::kMaxDiagRun, {st, e});
+						sums.add(blocks, tqb::kMaxDiagRun, {false, std::move(col_op)});
 					}
 					e = st;
 				}

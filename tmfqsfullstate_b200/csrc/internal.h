@@ -198,6 +198,8 @@ unsigned launch_obs_apply(const LaunchCtx &c, int prec, const void *psi, void *l
                           const double *weights, unsigned nterms, double *dev_partials);
 // Angle-derivative sums of a diagonal run (partials[block * kMaxDiagRun + k]),
 // then the run's inverse on lambda (and on psi if asked); returns the blocks.
+// Entries that depend on index bits 0-2 (flips, masks with a bit there) placed
+// first, at most 8 of them, let the pass look up one phase table per amplitude.
 unsigned launch_grad_run(const LaunchCtx &c, int prec, void *lam, void *psi, unsigned n, const DiagEntry *entries,
                          unsigned count, bool uncompute_psi, double *dev_partials);
 
