@@ -356,6 +356,11 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 	};
 	// The first tile's copy starts before the tables are built.
 	uint64_t cbase = tile_base(blockIdx.x);
+	// Thread 0 computes the base of the tile after next one iteration ahead
+	// and hands it over through shared memory (the tile loop's barriers order
+	// the write before the reads).
+	__shared__ uint64_t nb_slot[2];
+	if(tid == 0 && blockIdx.x + gridDim.x < g.ntiles) nb_slot[0] = tile_base(blockIdx.x + gridDim.x);
 	prefetch(blockIdx.x, cbase, sh.buf[0], sh.Ot[0]);
 
 	for(unsigned k = tid; k < g.nstages; k += nthr) sh.stages[k] = gstages[k];
@@ -394,7 +399,8 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 	unsigned cur = 0;
 	for(uint64_t o = blockIdx.x; o < g.ntiles; o += gridDim.x, cur ^= 1u) {
 		const uint64_t next = o + gridDim.x;
-		const uint64_t nbase = next < g.ntiles ? tile_base(next) : cbase;
+		const uint64_t nbase = next < g.ntiles ? nb_slot[cur] : cbase;
+		if(tid == 0 && next + gridDim.x < g.ntiles) nb_slot[cur ^ 1u] = tile_base(next + gridDim.x);
 		prefetch(next, nbase, sh.buf[cur ^ 1u], sh.Ot[cur ^ 1u]);
 		const V *ot = sh.Ot[cur];
 		cp_async_wait1();
