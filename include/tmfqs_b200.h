@@ -265,8 +265,9 @@ TMFQS_API int tmfqs_sample_static(const void *device_amps, int precision, unsign
  * each run of consecutive diagonal ops (controlled phases, phase flips) gets
  * all its derivatives from one read of lambda and psi.  psi is checkpointed
  * every `checkpoint_every` ops of the forward pass (0: the smallest interval
- * whose checkpoints fit in half the free device memory) and restored from the
- * checkpoints in the backward pass, which bounds the complex64 drift of psi.
+ * whose checkpoints fit in half the free device memory); the backward pass
+ * takes psi of each segment from its checkpoint (un-computing it there, in
+ * place, where the segment needs it), which bounds the complex64 drift of psi.
  * Ops: H, X, CNOT, CPHASE, SWAP, PHASE_FLIP, GATE (INVERSION is rejected);
  * 1 <= obs_terms <= 64.  On return the handle holds the final state. */
 TMFQS_API int tmfqs_gpu_adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count,

@@ -1227,7 +1227,7 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 		sums.add(blocks, 1, {true, {}});
 	}
 
-	// Backward pass: segment by segment, psi restored from its checkpoint.
+	// Backward pass: segment by segment, psi taken from its checkpoint.
 	for(size_t sidx = nseg; sidx-- > 0;) {
 		const size_t a0 = sidx * K, b0 = std::min(count, a0 + K);
 		// cp_before[i - a0]: a controlled phase lies in [a0, i).
