@@ -306,6 +306,8 @@ struct Planner {
 	std::vector<unsigned> msched;  // fast forms: low-bit width of the first multi-op passes
 	unsigned mrest = 0;            // ... and of the passes after them
 	size_t npass = 0;              // multi-op passes run so far
+	void *mirror = nullptr;        // a radix pass launched by the next flush also writes its result here
+	bool mirrored = false;         // ... and did
 
 	explicit Planner(tmfqs_gpu_state *hh) : h(hh) {
 		// Tiles of 2^12 complex128 / 2^13 complex64 amplitudes (64 KB).  The
@@ -428,7 +430,9 @@ struct Planner {
 			                 tqb::launch_qft_pass(ctx(h), h->precision, h->amps, pass);
 			if(qft) ++h->stats.qft_passes;
 			const bool done = qft || (twiddle && h->opt_radix &&
-			                          tqb::launch_radix_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes));
+			                          tqb::launch_radix_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes,
+			                                                 mirror));
+			mirrored = !qft && done && mirror;
 			if(!done) tqb::launch_fused_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes);
 			++h->stats.fused_passes;
 		}
@@ -957,8 +961,10 @@ size_t run_dense_block(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t i, size_t
 
 // tmfqs_gpu_apply_ops: the Simulator's gate runs through the fusion planner.
 // With sync false the passes are left in flight on the handle's stream (the
-// caller synchronises and checks the device error word).
-void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool sync = true) {
+// caller synchronises and checks the device error word).  With `mirror` (a
+// state-sized buffer), returns whether the batch's last launch was a radix
+// pass that also wrote the final state there.
+bool apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool sync = true, void *mirror = nullptr) {
 	ensure_initialized(h, "operation batch");
 	if(count && !ops) fail(TMFQS_ERR_INVALID_ARGUMENT, "null op list");
 	DeviceScope d(h);
@@ -974,7 +980,7 @@ void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool 
 			check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
 			check_device_error(h);
 		}
-		return;
+		return false;
 	}
 	Planner p(h);
 	size_t i = 0;
@@ -1016,10 +1022,13 @@ void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool 
 			p.add(op);
 			++i;
 		}
+		p.mirror = mirror;
 		p.flush();
+		p.mirror = nullptr;
 	} catch(const tqb::Error &) {
 		// Ops before the failing one are applied, as in the reference's
 		// sequential loop (simulator.cpp:72-82).
+		p.mirror = nullptr;
 		p.flush();
 		throw;
 	}
@@ -1027,6 +1036,7 @@ void apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool 
 		check_cuda(cudaStreamSynchronize(h->stream), "apply_ops sync");
 		check_device_error(h);
 	}
+	return p.mirrored;
 }
 
 // ---- adjoint gradient (tmfqs_gpu_adjoint_gradient) ----
@@ -1215,8 +1225,10 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 	// Forward pass, with psi saved after every segment of K ops.
 	for(size_t sidx = 0; sidx < nseg; ++sidx) {
 		const size_t a0 = sidx * K, len = std::min(K, count - a0);
-		apply_ops_body(h, ops + a0, len, false);
-		check_cuda(cudaMemcpyAsync(ckb + sidx * bytes, h->amps, bytes, cudaMemcpyDeviceToDevice, h->stream), "checkpoint");
+		// The segment's last pass writes the checkpoint as well when it is a
+		// radix pass; otherwise the state is copied.
+		if(!apply_ops_body(h, ops + a0, len, false, ckb + sidx * bytes))
+			check_cuda(cudaMemcpyAsync(ckb + sidx * bytes, h->amps, bytes, cudaMemcpyDeviceToDevice, h->stream), "checkpoint");
 	}
 
 	{

@@ -167,8 +167,9 @@ void launch_fused_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &p
 // Radix-2^RB form of a fused pass for the fast forms (complex64, or complex128
 // without exact arithmetic): programs of H, H-chains, twiddles and controlled
 // phases.  Returns false (nothing launched) when the pass does not qualify.
+// With `mirror` (a state-sized buffer) the pass also writes its result there.
 bool launch_radix_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, void *&dev_prog,
-                       size_t &dev_prog_bytes);
+                       size_t &dev_prog_bytes, void *mirror = nullptr);
 
 // The dedicated pass for a segment of the QFT ladder (Hadamards on consecutive
 // descending bits, each followed by the phases pi/2^(b-c) with every lower bit

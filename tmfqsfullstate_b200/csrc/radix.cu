@@ -294,7 +294,8 @@ namespace {
 template <typename R, int RB>
 __global__ void __launch_bounds__(kRadixThreads, 1)
 	k_radix(typename Vec2<R>::type *a, RadixGeom g, const unsigned char *prog, size_t off_stages, size_t off_items,
-	        size_t off_tabs, size_t off_slots, size_t off_terms, const typename Vec2<R>::type *otab, unsigned ot_stride) {
+	        size_t off_tabs, size_t off_slots, size_t off_terms, const typename Vec2<R>::type *otab, unsigned ot_stride,
+	        typename Vec2<R>::type *mirror) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const unsigned T = 1u << g.K;
@@ -461,6 +462,7 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 					for(int i = 0; i < RB; ++i)
 						if((r >> i) & 1) x |= gbit[i];
 					a[x] = v[r];
+					if(mirror) mirror[x] = v[r];
 				}
 			} else {
 				// Each thread rewrites only the slots it read in this stage.
@@ -470,8 +472,10 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 				if(last)
 					for(unsigned q = tid; q < T / per16; q += nthr) {
 						const unsigned j = q * per16;
-						*reinterpret_cast<float4 *>(a + (cbase | scatter(j))) =
-							*reinterpret_cast<const float4 *>(tile + rswz<V>(j));
+						const uint64_t x = cbase | scatter(j);
+						const float4 w = *reinterpret_cast<const float4 *>(tile + rswz<V>(j));
+						*reinterpret_cast<float4 *>(a + x) = w;
+						if(mirror) *reinterpret_cast<float4 *>(mirror + x) = w;
 					}
 			}
 		}
@@ -825,7 +829,7 @@ size_t radix_smem_bytes(size_t vbytes, const RadixGeom &g) {
 }
 
 template <typename R, int RB>
-bool run_radix(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_prog, size_t &dev_prog_bytes) {
+bool run_radix(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_prog, size_t &dev_prog_bytes, void *mirror) {
 	typedef typename Vec2<R>::type V;
 	const unsigned K = pass.K;
 	if(K < (unsigned)RB + 5 || K > 13 || (1u << (K - RB)) > kRadixThreads) return false;
@@ -885,7 +889,7 @@ bool run_radix(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	const uint64_t grid = std::min<uint64_t>(P.g.ntiles, (uint64_t)c.num_sms);
 	k_radix<R, RB><<<(unsigned)grid, threads, smem, c.stream>>>(static_cast<V *>(a), P.g,
 	                                                           static_cast<const unsigned char *>(dev_prog), o_st, o_it,
-	                                                           o_tb, o_sl, o_tm, otab, ot_stride);
+	                                                           o_tb, o_sl, o_tm, otab, ot_stride, static_cast<V *>(mirror));
 	check_cuda(cudaGetLastError(), "radix pass");
 	if(c.launches) ++*c.launches;
 	return true;
@@ -894,9 +898,9 @@ bool run_radix(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 }  // namespace
 
 bool launch_radix_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, void *&dev_prog,
-                       size_t &dev_prog_bytes) {
-	if(prec == TMFQS_FP64) return run_radix<double, 3>(c, a, pass, dev_prog, dev_prog_bytes);
-	return run_radix<float, 4>(c, a, pass, dev_prog, dev_prog_bytes);
+                       size_t &dev_prog_bytes, void *mirror) {
+	if(prec == TMFQS_FP64) return run_radix<double, 3>(c, a, pass, dev_prog, dev_prog_bytes, mirror);
+	return run_radix<float, 4>(c, a, pass, dev_prog, dev_prog_bytes, mirror);
 }
 
 }  // namespace tqb
