@@ -455,15 +455,18 @@ __global__ void __launch_bounds__(kRadixThreads, 1)
 				uint64_t gbit[RB];
 #pragma unroll
 				for(int i = 0; i < RB; ++i) gbit[i] = S.gbit[i];
+				auto store = [&](V *dst) {
 #pragma unroll
-				for(int r = 0; r < (1 << RB); ++r) {
-					uint64_t x = gt;
+					for(int r = 0; r < (1 << RB); ++r) {
+						uint64_t x = gt;
 #pragma unroll
-					for(int i = 0; i < RB; ++i)
-						if((r >> i) & 1) x |= gbit[i];
-					a[x] = v[r];
-					if(mirror) mirror[x] = v[r];
-				}
+						for(int i = 0; i < RB; ++i)
+							if((r >> i) & 1) x |= gbit[i];
+						dst[x] = v[r];
+					}
+				};
+				store(a);
+				if(mirror) store(mirror);
 			} else {
 				// Each thread rewrites only the slots it read in this stage.
 #pragma unroll
