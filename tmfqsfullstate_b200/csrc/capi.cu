@@ -1285,10 +1285,22 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 					e = st;
 				}
 			} else {
-				// Inverse of the run, last op first.
+				// Inverse of the run, last op first.  A run of Hadamards and X gates
+				// on distinct qubits commutes and each op is its own inverse: it is
+				// un-applied in circuit order, which the planner packs into the same
+				// passes as the forward (a layer's Hadamards from the top qubit down).
+				bool commuting = true;
+				uint64_t seen = 0;
+				for(size_t k = j; k < i && commuting; ++k) {
+					const tmfqs_op &op = ops[k];
+					const uint64_t q = 1ull << bit_of(h, op.q0);
+					commuting = (op.kind == TMFQS_OP_H || op.kind == TMFQS_OP_X) && !(seen & q);
+					seen |= q;
+				}
 				std::vector<tmfqs_op> inv;
 				std::vector<std::vector<double>> mats;
-				for(size_t k = i; k-- > j;) {
+				for(size_t s = 0; s < i - j; ++s) {
+					const size_t k = commuting ? j + s : i - 1 - s;
 					tmfqs_op op = ops[k];
 					if(op.kind == TMFQS_OP_GATE) {
 						const size_t dim = size_t(1) << op.k;
