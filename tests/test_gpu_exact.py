@@ -240,6 +240,28 @@ def test_fused_random_circuits_bitexact(gpu, seed):
     assert_same(got, ref, f"random circuit seed={seed}")
 
 
+def test_long_diagonal_pass_bitexact(gpu):
+    """1500 diagonal ops in one fused pass: its program (84 KB) is larger than
+    a pinned upload slot and goes up synchronously; the next batches reuse the
+    slots."""
+    n = 10
+    rng = np.random.default_rng(99)
+    ops = [tq.h(q) for q in range(n)]
+    for _ in range(1500):
+        q = [int(v) for v in rng.permutation(n)[:2]]
+        if rng.random() < 0.8:
+            ops.append(tq.cphase(q[0], q[1], float(rng.uniform(-4, 4))))
+        else:
+            ops.append(tq.phase_flip(int(rng.integers(0, 1 << n))))
+    ops += [tq.h(q) for q in range(n)]
+    a = rand_state(n, 98)
+    for rep in range(2):
+        got, ref = ops_equal_run(gpu, n, a, ops)
+        assert_same(got, ref, f"long diagonal pass, run {rep}")
+        small, sref = ops_equal_run(gpu, n, a, tq.qft_ops(n))
+        assert_same(small, sref, f"QFT after the long pass, run {rep}")
+
+
 def test_apply_ops_error_leaves_prefix_applied(gpu):
     n = 4
     a = rand_state(n, 8)
