@@ -1,0 +1,102 @@
+// Host-side check of the QFT segment recogniser and planner (qft_segment and
+// plan_qft in tmfqsfullstate_b200/csrc/qft_pass.cu): one line per constructed
+// pass, for tests/test_qft_plan.py.  No GPU is touched.
+#include "../tmfqsfullstate_b200/csrc/qft_pass.cu"
+
+#include <cstdio>
+#include <cstdlib>
+
+namespace tqb {
+[[noreturn]] void fail(int, const std::string &m) {
+	std::fprintf(stderr, "%s\n", m.c_str());
+	std::exit(2);
+}
+void check_cuda(cudaError_t, const char *) {}
+}  // namespace tqb
+
+using namespace tqb;
+
+// A pass of n qubits over the given local bits: Hadamards on the bits of `hs`
+// (descending), each followed by the ladder's phases pi/2^(b-c) for c in
+// [r0, b).  `drop` removes the last phase of the first chain, `skew` changes
+// the first chain's first angle, `bare` leaves the Hadamards without phases.
+static FusedPass make(unsigned n, const std::vector<unsigned> &local, const std::vector<unsigned> &hs, unsigned r0,
+                      bool drop = false, bool skew = false, bool bare = false) {
+	FusedPass p;
+	p.n = n;
+	p.K = (unsigned)local.size();
+	for(unsigned i = 0; i < p.K; ++i) p.lpos[i] = local[i];
+	auto li = [&](unsigned bit) -> int {
+		for(unsigned i = 0; i < p.K; ++i)
+			if(p.lpos[i] == bit) return (int)i;
+		return -1;
+	};
+	const double pi = std::acos(-1.0);
+	for(size_t k = 0; k < hs.size(); ++k) {
+		const unsigned b = hs[k];
+		FusedOp f{};
+		f.lt = (unsigned)li(b);
+		if(bare) {
+			f.kind = kFH;
+			p.ops.push_back(f);
+			continue;
+		}
+		f.kind = kFHChain;
+		f.tab = (uint32_t)p.chain.size();
+		unsigned cnt = 0;
+		for(int c = (int)b - 1; c >= (int)r0; --c) {
+			if(drop && k == 0 && c == (int)r0) break;
+			double th = std::ldexp(pi, -(int)(b - (unsigned)c));
+			if(skew && k == 0 && cnt == 0) th *= 1.001;
+			p.chain.push_back(ChainEntry{std::cos(th), std::sin(th), th, li((unsigned)c), (unsigned)c});
+			++cnt;
+		}
+		f.lc = cnt;
+		if(cnt == 0) f.kind = kFH;
+		p.ops.push_back(f);
+	}
+	return p;
+}
+
+static void check(const char *name, const FusedPass &p) {
+	std::vector<unsigned> hb;
+	unsigned r0 = 0;
+	const bool seg = qft_segment(p, hb, r0);
+	int planned = -1;
+	unsigned nstages = 0;
+	double scale = 0.0;
+	if(seg) {
+		QftGeom g{};
+		planned = plan_qft(p, hb, r0, 8, 5, g) ? 1 : 0;
+		nstages = g.nstages;
+		scale = g.scale;
+	}
+	std::printf("case %s segment %d hb %zu r0 %u planned %d nstages %u scale %.17g\n", name, (int)seg, hb.size(), seg ? r0 : 0u,
+	            planned, nstages, scale);
+}
+
+static std::vector<unsigned> range(unsigned lo, unsigned hi) {  // [lo, hi)
+	std::vector<unsigned> v;
+	for(unsigned b = lo; b < hi; ++b) v.push_back(b);
+	return v;
+}
+static std::vector<unsigned> down(unsigned hi, unsigned lo) {  // hi, hi-1, ..., lo
+	std::vector<unsigned> v;
+	for(int b = (int)hi; b >= (int)lo; --b) v.push_back((unsigned)b);
+	return v;
+}
+
+int main() {
+	// 28 qubits, complex64: the planner's passes hold bits {0..4} and the
+	// pass's Hadamard bits, then the last pass the 13 lowest bits.
+	std::vector<unsigned> first = range(0, 5), top = range(20, 28);
+	first.insert(first.end(), top.begin(), top.end());
+	check("qft28_first", make(28, first, down(27, 20), 0));
+	check("qft28_last", make(28, range(0, 13), down(11, 0), 0));
+	check("lone_h", make(28, range(0, 13), {7}, 0, false, false, true));
+	check("bare_run", make(28, range(0, 13), down(7, 4), 0, false, false, true));
+	check("dropped_phase", make(28, range(0, 13), down(11, 0), 0, true));
+	check("wrong_angle", make(28, range(0, 13), down(11, 0), 0, false, true));
+	check("sub_register", make(20, range(0, 13), down(12, 6), 3));
+	return 0;
+}

@@ -1,0 +1,49 @@
+"""The QFT segment recogniser and planner on the host (CPU only), through
+tests/qft_plan_check.cu: which passes run as QFT segments, their stage
+counts and their real scale (1/sqrt(2))^P."""
+import math
+import os
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def cases(tmp_path_factory):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    exe = str(tmp_path_factory.mktemp("qft") / "qft_plan_check")
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=compute_100a", "-std=c++17", "--expt-relaxed-constexpr",
+                    "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "tmfqsfullstate_b200", "csrc"),
+                    "-o", exe, os.path.join(ROOT, "tests", "qft_plan_check.cu")], check=True, timeout=600)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True, timeout=60).stdout
+    res = {}
+    for line in out.splitlines():
+        f = line.split()
+        res[f[1]] = {"segment": int(f[3]), "hb": int(f[5]), "r0": int(f[7]), "planned": int(f[9]),
+                     "nstages": int(f[11]), "scale": float(f[13])}
+    return res
+
+
+@pytest.mark.parametrize("name,hadamards,stages,r0", [("qft28_first", 8, 2, 0), ("qft28_last", 12, 3, 0),
+                                                     ("sub_register", 7, 2, 3)])
+def test_ladder_passes_are_planned(cases, name, hadamards, stages, r0):
+    c = cases[name]
+    assert c["segment"] == 1 and c["planned"] == 1
+    assert c["hb"] == hadamards and c["r0"] == r0 and c["nstages"] == stages
+    assert math.isclose(c["scale"], 0.5 ** (hadamards / 2), rel_tol=1e-15)
+
+
+def test_lone_hadamard_is_a_segment(cases):
+    assert cases["lone_h"]["segment"] == 1 and cases["lone_h"]["planned"] == 1 and cases["lone_h"]["nstages"] == 1
+
+
+@pytest.mark.parametrize("name", ["bare_run", "dropped_phase", "wrong_angle"])
+def test_non_ladders_are_rejected(cases, name):
+    """Hadamard runs without their phases, a chain missing a phase, and a
+    wrong angle go to the general radix pass."""
+    assert cases[name]["segment"] == 0

@@ -22,7 +22,7 @@ def plans(tmp_path_factory):
     if not os.path.exists(nvcc):
         pytest.skip("nvcc not available")
     exe = str(tmp_path_factory.mktemp("radix") / "radix_plan_check")
-    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "--expt-relaxed-constexpr",
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=compute_100a", "-std=c++17", "--expt-relaxed-constexpr",
                     "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "tmfqsfullstate_b200", "csrc"),
                     "-o", exe, os.path.join(ROOT, "tests", "radix_plan_check.cu")], check=True, timeout=600)
     out = subprocess.run([exe], capture_output=True, text=True, check=True, timeout=60).stdout
