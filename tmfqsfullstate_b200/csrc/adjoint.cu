@@ -118,9 +118,12 @@ __global__ void __launch_bounds__(kAdjThreads) k_obs_apply(const typename Vec2<R
 //
 // The inverse of the run multiplies amplitude x by the product of the
 // conjugate phases of its hit entries (-1 for a flip).  The gates commute, so
-// the product is taken byte by byte over the hit word: four tables of 256
-// products (formed in FP64, rounded once to the storage type) and at most
-// three complex products per amplitude.
+// the product is taken byte by byte over the hit word: up to four tables of
+// 256 products (formed in FP64, rounded once to the storage type).  When the
+// caller put the entries that depend on index bits 0-2 first and there are at
+// most 8 of them, bytes 1-3 of the hit word are the same for a thread's eight
+// amplitudes: their product is formed once per batch, and each amplitude takes
+// one lookup and one complex product for its phase.
 //
 // Gradients: a thread owns kGradBatch = 8 consecutive amplitudes x0 + u, so
 // for a controlled phase with mask m the condition splits into its low part
