@@ -247,10 +247,14 @@ TMFQS_API int tmfqs_gpu_grover_run(tmfqs_gpu_state *h, tmfqs_register_view *view
  * and a host pointer for the index; the function allocates nothing.  Its
  * working tables live in a fixed 2 MiB device array inside the library, so
  * states are limited to num_qubits <= 24 (larger ones return
- * TMFQS_ERR_INVALID_ARGUMENT).  The first call on each device looks up that
- * array's device address (cudaGetSymbolAddress): make it before any stream
- * capture.  All calls share the array -- calls that overlap on the GPU race --
- * and each call returns after the result is on the host. */
+ * TMFQS_ERR_INVALID_ARGUMENT).  Every call made outside stream capture looks
+ * up that array's device address (cudaGetSymbolAddress), so a context reset
+ * (cudaDeviceReset, which may reload the library's module elsewhere) is picked
+ * up by the next such call; a call on a capturing stream reuses the address
+ * of the last call outside capture on that device, so the first call on each
+ * device -- and the first after a reset -- must come before any stream capture
+ * (otherwise TMFQS_ERR_LOGIC).  All calls share the array -- calls that overlap
+ * on the GPU race -- and each call returns after the result is on the host. */
 TMFQS_API int tmfqs_sample_static(const void *device_amps, int precision, unsigned num_qubits, double rnd,
                                   void *stream, uint64_t *index_out);
 /* The differentiation form (no reference counterpart; its checks use the

@@ -24,7 +24,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(_HERE, "liboracle.so")
 REF_SO = os.path.join(_HERE, "_ref", "libtmfqs_ref.so")
-REFERENCE_SRC = "/root/reference"
+# Where the reference sources are, for building _ref/; unset, the Makefile's own default is used.
+REFERENCE_SRC = os.environ.get("TMFQS_REFERENCE_SRC")
 
 OP_H, OP_X, OP_CNOT, OP_CPHASE, OP_SWAP, OP_GATE, OP_PHASE_FLIP, OP_INVERSION = range(8)
 ERRORS = {1: IndexError, 2: ValueError, 3: RuntimeError, 4: RuntimeError, 5: MemoryError}
@@ -66,7 +67,8 @@ class _Reg(ctypes.Structure):
 
 def build() -> None:
     """Compile liboracle.so and, when the reference sources exist, _ref/."""
-    subprocess.run(["make", "-s", "-C", _HERE, f"REF={REFERENCE_SRC}"], check=True)
+    extra = [f"REF={REFERENCE_SRC}"] if REFERENCE_SRC else []
+    subprocess.run(["make", "-s", "-C", _HERE] + extra, check=True)
 
 
 _lib = None

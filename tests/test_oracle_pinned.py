@@ -153,3 +153,30 @@ def test_oracle_matches_reference_inputs_and_builders():
         assert [(o.kind, o.q0, o.q1, o.theta) for o in a] == [(o.kind, o.q0, o.q1, o.theta) for o in b]
     a, b = O.grover_ops(6, [9, 3, 9], True), O.ref_grover_ops(6, [9, 3, 9], True)
     assert [(o.kind, o.q0, o.state, o.materialized) for o in a] == [(o.kind, o.q0, o.state, o.materialized) for o in b]
+
+
+def test_product_input_generator_matches_golden_digests():
+    """tmfqs_random_phase (the product's host input generator) against the
+    reference's QuantumState::randomPhase (src/tmfqs/state/quantum_state.cpp:264-277),
+    through the committed digests of the reference's own inputs."""
+    import tmfqsfullstate_b200 as tq
+
+    for n in (12, 16):
+        assert digest(tq.random_phase(n, 123456)) == GOLDEN[f"qft{n}_random_phase"]["input_sha256"]
+
+
+def test_product_input_generator_matches_golden_qft28_digest():
+    """The 28-qubit bench input, bit for bit (4 GiB on the host, about 15 s)."""
+    import tmfqsfullstate_b200 as tq
+
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "qft28_ref.json")))
+    assert digest(tq.random_phase(28, gold["seed"])) == gold["input_sha256"]
+
+
+@needs_ref
+@pytest.mark.parametrize("n,seed", [(1, 0), (3, 5), (10, 99), (14, 123456), (17, 4242)])
+def test_product_input_generator_matches_reference(n, seed):
+    import tmfqsfullstate_b200 as tq
+
+    assert np.array_equal(tq.random_phase(n, seed), O.RefState(n, "random_phase", seed=seed).amplitudes())
+    assert np.array_equal(tq.mt19937_unit(seed, 100), O.ref_mt_unit(seed, 100))

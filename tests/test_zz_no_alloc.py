@@ -21,21 +21,22 @@ import tmfqsfullstate_b200 as tq
 pytestmark = pytest.mark.gpu
 
 
-def _prepared_state(n, seed):
-    g = tq.GpuState(tq.FP64)
+def _prepared_state(n, seed, prec=tq.FP64):
+    g = tq.GpuState(prec)
     g.load(n, tq.random_phase(n, seed))
     g.apply_ops(tq.qft_ops(n))
     return g
 
 
+@pytest.mark.parametrize("prec", [tq.FP64, tq.FP32])
 @pytest.mark.parametrize("n", [1, 12, 20, 24])
-def test_static_sample_matches_handle_sample_twice_in_a_row(n):
-    with _prepared_state(n, 123 + n) as g:
+def test_static_sample_matches_handle_sample_twice_in_a_row(n, prec):
+    with _prepared_state(n, 123 + n, prec) as g:
         ptr, nbytes = g.device_buffer()
-        assert nbytes == 16 << n
+        assert nbytes == (16 if prec == tq.FP64 else 8) << n
         stream = g.stream()
         draws = [float(v) for v in tq.mt19937_unit(123456 + n, 2)]
-        got = [tq.sample_static(ptr, tq.FP64, n, r, stream) for r in draws]
+        got = [tq.sample_static(ptr, prec, n, r, stream) for r in draws]
         want = [g.sample(r) for r in draws]
         assert got == want
 

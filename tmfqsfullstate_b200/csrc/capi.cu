@@ -248,6 +248,15 @@ void write_amp(tmfqs_gpu_state *h, uint64_t s, double re, double im) {
 	h->dirty[s] = true;
 }
 
+// Like write_amp, but the cache keeps the FP64 value: a complex64 state then
+// rounds it once, when it is flushed to the device, instead of at every
+// register update (the lazy Grover flips rewrite the same few amplitudes once
+// per iteration).  Identical to write_amp for complex128.
+void carry_amp(tmfqs_gpu_state *h, uint64_t s, double re, double im) {
+	h->cache[s] = {re, im};
+	h->dirty[s] = true;
+}
+
 // Host <-> device copies of interleaved complex128 data, converting for
 // complex64 states through a device staging buffer.
 void copy_in(tmfqs_gpu_state *h, uint64_t first, const double *host, uint64_t count) {
@@ -778,13 +787,13 @@ void register_flip(tmfqs_gpu_state *h, tmfqs_register_view *v, uint64_t s) {
 		}
 		if(v->overlay) {
 			const Cx nb = overlay_remove(*v, cneg(logical));
-			write_amp(h, s, nb.re, nb.im);
+			carry_amp(h, s, nb.re, nb.im);
 			return;
 		}
 	}
 	auto it = h->cache.find(s);
 	if(it != h->cache.end()) {
-		write_amp(h, s, -it->second.first, -it->second.second);
+		carry_amp(h, s, -it->second.first, -it->second.second);
 		return;
 	}
 	flush_dirty(h);

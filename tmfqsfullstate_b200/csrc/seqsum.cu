@@ -606,16 +606,25 @@ std::mutex g_static_mutex;
 void *g_static_addr[64] = {nullptr};  // device address of g_static_scratch, per device ordinal
 
 // Host code cannot use &g_static_scratch as a device address; the runtime
-// gives the real address for the current device.
-void *static_scratch_address() {
+// gives the real address for the current device.  It is looked up again on
+// every call made outside stream capture: a context reset (cudaDeviceReset)
+// reloads the module, and the array may then sit at another address.  While
+// `stream` is capturing, the address of the last call outside capture on this
+// device is used (no lookup, which could load the module inside a capture);
+// a capturing call on a device that never had one fails.
+void *static_scratch_address(cudaStream_t stream) {
 	int dev = 0;
 	check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
 	if(dev < 0 || dev >= 64) fail(TMFQS_ERR_INVALID_ARGUMENT, "device ordinal out of range for the static scratch");
+	cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+	check_cuda(cudaStreamIsCapturing(stream, &cap), "cudaStreamIsCapturing");
 	std::lock_guard<std::mutex> lock(g_static_mutex);
-	if(!g_static_addr[dev]) {
+	if(cap == cudaStreamCaptureStatusNone) {
 		void *p = nullptr;
 		check_cuda(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress(static scratch)");
 		g_static_addr[dev] = p;
+	} else if(!g_static_addr[dev]) {
+		fail(TMFQS_ERR_LOGIC, "tmfqs_sample_static: the first call on a device must come before any stream capture");
 	}
 	return g_static_addr[dev];
 }
@@ -666,7 +675,7 @@ SeqResult seq_sample_static(int precision, const void *amps, unsigned num_qubits
 	check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
 	WalkOut host{};  // pageable: the readback copy is synchronous
 	SeqScratch s;
-	carve_static(s, N, static_scratch_address(), &host);
+	carve_static(s, N, static_scratch_address(stream), &host);
 	if(precision == TMFQS_FP64) return run_engine<double, kTermProb>(amps, N, Overlay{}, true, rnd, s, stream, sms, nullptr);
 	return run_engine<float, kTermProb>(amps, N, Overlay{}, true, rnd, s, stream, sms, nullptr);
 }
