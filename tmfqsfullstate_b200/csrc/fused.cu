@@ -37,8 +37,69 @@ struct FusedGeom {
 	unsigned lpos[kMaxLocal];  // ascending local bit positions
 	uint64_t ntiles;
 	unsigned nops;
+	unsigned sw;               // shared-memory swizzle: slot of local index j is j ^ ((j >> sw) & 7)
 	double inv;                // 1.0 / std::sqrt(2.0), formed on the host (dense_state_backend.cpp:258)
 };
+
+// Thread layout of one H-chain op of a pass with K >= 7 local bits, built on
+// the host (build_chain_map).  The op's 2^(K-1) butterflies are numbered by a
+// pair index p = lane + 32 q; p's bits map to the local bits other than the
+// Hadamard's in an order chosen so that a warp's lanes differ, where possible,
+// only in bits that are no control of the chain.  A controlled phase whose
+// control is not a lane bit is then applied by all lanes of a warp or by
+// none: the per-amplitude loop over the set controls does not diverge, and
+// skipped phases cost no issue slots.  Entry e of the chain is bit 63 - e of
+// a mask.  The three lowest lane bits are, for each i < 3, local bit i or
+// local bit K-3+i: with the swizzle j ^ ((j >> (K-3)) & 7) the 16-byte shared
+// accesses of each quarter-warp then hit distinct banks.
+struct ChainMap {
+	uint64_t ml[32];   // per lane: the chain entries whose control is set in its offset
+	uint64_t mr[128];  // per warp-iteration q: the same for its offset
+	uint16_t jl[32];   // per lane: local index offset
+	uint16_t jr[128];  // per q: local index offset
+	uint32_t nq;       // number of q values, 2^(K-6)
+	uint32_t ilp;      // 1: bit 0 of q is no control, so q and q+1 share their mask
+	uint32_t pad[2];
+};
+constexpr uint64_t kNoChainMap = ~0ull;
+
+// Applies the chain entries of mask m (entry e = bit 63-e, ascending e =
+// circuit order) to one amplitude: each a separately rounded complex product
+// (dense_state_backend.cpp:300-301), exactly as the per-gate path.
+template <typename R>
+__device__ __forceinline__ void chain_apply(uint64_t m, const double2 *cph, R &r, R &i) {
+	for(uint32_t hi = (uint32_t)(m >> 32); hi;) {
+		const unsigned e = __clz(hi);
+		hi ^= 0x80000000u >> e;
+		const double2 ph = cph[e];
+		cmul_ref((R)ph.x, (R)ph.y, r, i);
+	}
+	for(uint32_t lo = (uint32_t)m; lo;) {
+		const unsigned e = __clz(lo);
+		lo ^= 0x80000000u >> e;
+		const double2 ph = cph[32 + e];
+		cmul_ref((R)ph.x, (R)ph.y, r, i);
+	}
+}
+
+// The same for two amplitudes with the same mask.
+template <typename R>
+__device__ __forceinline__ void chain_apply2(uint64_t m, const double2 *cph, R &ra, R &ia, R &rb, R &ib) {
+	for(uint32_t hi = (uint32_t)(m >> 32); hi;) {
+		const unsigned e = __clz(hi);
+		hi ^= 0x80000000u >> e;
+		const double2 ph = cph[e];
+		cmul_ref((R)ph.x, (R)ph.y, ra, ia);
+		cmul_ref((R)ph.x, (R)ph.y, rb, ib);
+	}
+	for(uint32_t lo = (uint32_t)m; lo;) {
+		const unsigned e = __clz(lo);
+		lo ^= 0x80000000u >> e;
+		const double2 ph = cph[32 + e];
+		cmul_ref((R)ph.x, (R)ph.y, ra, ia);
+		cmul_ref((R)ph.x, (R)ph.y, rb, ib);
+	}
+}
 
 __device__ __forceinline__ uint64_t expand_outer(uint64_t o, const FusedGeom &g) {
 	for(unsigned i = 0; i < g.K; ++i) o = insert0(o, g.lpos[i]);
@@ -65,8 +126,8 @@ __device__ __forceinline__ bool butterfly(typename Vec2<R>::type &x, typename Ve
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type *a, FusedGeom g, const FusedOp *ops,
-                                                         const ChainEntry *chain) {
+__global__ void __launch_bounds__(kFusedThreads, 3) k_fused(typename Vec2<R>::type *a, FusedGeom g, const FusedOp *ops,
+                                                            const ChainEntry *chain, const ChainMap *maps) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ unsigned char smem_raw[];
 	const unsigned T = 1u << g.K;
@@ -79,6 +140,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 	__shared__ double2 cph[64];
 	__shared__ int cloc[64];
 	__shared__ unsigned ccount;
+	__shared__ uint64_t cu;  // mapped chains: entries whose control is an outer bit set in this tile
 	// Twiddle form: table A (outer phase x first 6 local controls) and table B
 	// (next 5 local controls), built per tile in FP64.
 	__shared__ double2 twa[64], twb[32];
@@ -99,11 +161,13 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 	const unsigned lane = threadIdx.x & 31u;
 	const unsigned lowmask = (1u << g.m) - 1u;
 	auto scatter = [&](unsigned j) -> uint64_t { return (uint64_t)(j & lowmask) | hitab[j >> g.m]; };
+	// Shared slot of local index j (swizzled; the identity for small tiles).
+	auto P = [&](unsigned j) -> unsigned { return j ^ ((j >> g.sw) & 7u); };
 	const unsigned half = T >> 1, quarter = T >> 2;
 	const R inv = (R)g.inv;
 	for(uint64_t o = blockIdx.x; o < g.ntiles; o += gridDim.x) {
 		const uint64_t base = expand_outer(o, g);
-		for(unsigned j = threadIdx.x; j < T; j += blockDim.x) s[j] = a[base | scatter(j)];
+		for(unsigned j = threadIdx.x; j < T; j += blockDim.x) s[P(j)] = a[base | scatter(j)];
 		__syncthreads();
 		for(unsigned k = 0; k < g.nops; ++k) {
 			const FusedOp op = ops[k];
@@ -111,15 +175,87 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 				case kFH: {
 					for(unsigned p = threadIdx.x; p < half; p += blockDim.x) {
 						const unsigned j0 = (unsigned)insert0(p, op.lt), j1 = j0 | (1u << op.lt);
-						V x = s[j0], y = s[j1];
+						V x = s[P(j0)], y = s[P(j1)];
 						if(!butterfly<R>(x, y, inv)) continue;
-						s[j0] = x;
-						s[j1] = y;
+						s[P(j0)] = x;
+						s[P(j1)] = y;
 					}
 					__syncthreads();
 					break;
 				}
 				case kFHChain: {
+					if(op.state != kNoChainMap) {
+						// Phases of all entries, and the outer-controlled entries that
+						// apply in this tile (every |1> output gets them).
+						if(threadIdx.x < 32) {
+							uint64_t u = 0;
+							for(unsigned e0 = 0; e0 < op.lc; e0 += 32) {
+								const unsigned e = e0 + lane;
+								bool on = false;
+								if(e < op.lc) {
+									const ChainEntry ce = chain[op.tab + e];
+									cph[e] = make_double2(ce.cr, ce.ci);
+									on = ce.local < 0 && ((base >> ce.bit) & 1ull);
+								}
+								const unsigned b = __ballot_sync(0xffffffffu, on);
+								u |= (uint64_t)__brev(b) << (e0 == 0 ? 32 : 0);
+							}
+							if(lane == 0) cu = u;
+						}
+						__syncthreads();
+						const ChainMap &cm = maps[op.state];
+						const unsigned tb = 1u << op.lt, jl = cm.jl[lane];
+						const uint64_t mlane = cm.ml[lane] | cu;
+						const unsigned warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+						if(cm.ilp) {
+							// Two butterflies per thread whose |1> outputs take the same
+							// phases (they differ in a bit that is no control).
+							for(unsigned q = 2 * warp; q < cm.nq; q += 2 * nw) {
+								const unsigned ja = jl | cm.jr[q], jb = jl | cm.jr[q + 1];
+								const uint64_t m = mlane | cm.mr[q];
+								V xa = s[P(ja)], ya = s[P(ja | tb)], xb = s[P(jb)], yb = s[P(jb | tb)];
+								const bool wa = butterfly<R>(xa, ya, inv), wb = butterfly<R>(xb, yb, inv);
+								// A zero |1> output is left alone by every phase (dense_state_backend.cpp:299).
+								const bool ca = wa && !is_zero<R>(ya), cb = wb && !is_zero<R>(yb);
+								if(ca || cb) {
+									R ra = ya.x, ia = ya.y, rb = yb.x, ib = yb.y;
+									chain_apply2<R>(m, cph, ra, ia, rb, ib);
+									if(ca) {
+										ya.x = ra;
+										ya.y = ia;
+									}
+									if(cb) {
+										yb.x = rb;
+										yb.y = ib;
+									}
+								}
+								if(wa) {
+									s[P(ja)] = xa;
+									s[P(ja | tb)] = ya;
+								}
+								if(wb) {
+									s[P(jb)] = xb;
+									s[P(jb | tb)] = yb;
+								}
+							}
+						} else {
+							for(unsigned q = warp; q < cm.nq; q += nw) {
+								const unsigned ja = jl | cm.jr[q];
+								V x = s[P(ja)], y = s[P(ja | tb)];
+								if(!butterfly<R>(x, y, inv)) continue;
+								if(!is_zero<R>(y)) {
+									R r = y.x, i = y.y;
+									chain_apply<R>(mlane | cm.mr[q], cph, r, i);
+									y.x = r;
+									y.y = i;
+								}
+								s[P(ja)] = x;
+								s[P(ja | tb)] = y;
+							}
+						}
+						__syncthreads();
+						break;
+					}
 					if(threadIdx.x < 32) {
 						unsigned pos = 0;
 						for(unsigned e0 = 0; e0 < op.lc; e0 += 32) {
@@ -149,7 +285,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 						const bool has1 = p1 < half;
 						const unsigned j00 = (unsigned)insert0(p0, op.lt), j01 = j00 | (1u << op.lt);
 						const unsigned j10 = has1 ? (unsigned)insert0(p1, op.lt) : j00, j11 = j10 | (1u << op.lt);
-						V x0 = s[j00], y0 = s[j01], x1 = s[j10], y1 = s[j11];
+						V x0 = s[P(j00)], y0 = s[P(j01)], x1 = s[P(j10)], y1 = s[P(j11)];
 						const bool w0 = butterfly<R>(x0, y0, inv);
 						const bool w1 = has1 && butterfly<R>(x1, y1, inv);
 						// A zero |1> output is left alone by every phase of the chain
@@ -178,12 +314,12 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 							}
 						}
 						if(w0) {
-							s[j00] = x0;
-							s[j01] = y0;
+							s[P(j00)] = x0;
+							s[P(j01)] = y0;
 						}
 						if(w1) {
-							s[j10] = x1;
-							s[j11] = y1;
+							s[P(j10)] = x1;
+							s[P(j11)] = y1;
 						}
 					}
 					__syncthreads();
@@ -238,7 +374,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 					const int na = tna, nb = tnb;
 					for(unsigned p = threadIdx.x; p < half; p += blockDim.x) {
 						const unsigned j0 = (unsigned)insert0(p, op.lt), j1 = j0 | (1u << op.lt);
-						V x = s[j0], y = s[j1];
+						V x = s[P(j0)], y = s[P(j1)];
 						if(!butterfly<R>(x, y, inv)) continue;
 						if(!is_zero<R>(y)) {
 							unsigned ia = 0, ib = 0;
@@ -253,8 +389,8 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 							y.x = nr;
 							y.y = ni;
 						}
-						s[j0] = x;
-						s[j1] = y;
+						s[P(j0)] = x;
+						s[P(j1)] = y;
 					}
 					__syncthreads();
 					break;
@@ -264,10 +400,10 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 					for(unsigned p = threadIdx.x; p < half; p += blockDim.x) {
 						const unsigned j0 = (unsigned)insert0(p, op.lt), j1 = j0 | (1u << op.lt);
 						if(op.kind == kFCnot && ((base | scatter(j0)) & op.mask) == 0) continue;
-						const V x = s[j0], y = s[j1];
+						const V x = s[P(j0)], y = s[P(j1)];
 						if(x.x == y.x && x.y == y.y) continue;
-						s[j0] = y;
-						s[j1] = x;
+						s[P(j0)] = y;
+						s[P(j1)] = x;
 					}
 					__syncthreads();
 					break;
@@ -277,9 +413,9 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 					for(unsigned q = threadIdx.x; q < quarter; q += blockDim.x) {
 						const unsigned j = (unsigned)insert00(q, lo, hi);
 						const unsigned ja = j | (1u << op.lt), jb = j | (1u << op.lc);
-						const V x = s[ja], y = s[jb];
-						s[ja] = y;
-						s[jb] = x;
+						const V x = s[P(ja)], y = s[P(jb)];
+						s[P(ja)] = y;
+						s[P(jb)] = x;
 					}
 					__syncthreads();
 					break;
@@ -300,7 +436,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 					__syncthreads();
 					for(unsigned j = threadIdx.x; j < T; j += blockDim.x) {
 						const uint64_t x = base | scatter(j);
-						V v = s[j];
+						V v = s[P(j)];
 						bool dirty = false;
 						for(unsigned q = 0; q < cnt; ++q) {
 							const uint64_t m = dmask[q];
@@ -316,7 +452,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 							}
 							dirty = true;
 						}
-						if(dirty) s[j] = v;
+						if(dirty) s[P(j)] = v;
 					}
 					// Diagonal ops keep the thread->amplitude ownership; the barrier
 					// also frees the staged chunk.
@@ -328,7 +464,7 @@ __global__ void __launch_bounds__(kFusedThreads) k_fused(typename Vec2<R>::type 
 					break;
 			}
 		}
-		for(unsigned j = threadIdx.x; j < T; j += blockDim.x) a[base | scatter(j)] = s[j];
+		for(unsigned j = threadIdx.x; j < T; j += blockDim.x) a[base | scatter(j)] = s[P(j)];
 		__syncthreads();
 	}
 }
@@ -581,6 +717,75 @@ void after_launch(const LaunchCtx &c, const char *what) {
 	if(c.launches) ++*c.launches;
 }
 
+// Thread layout of an H-chain op (see ChainMap): the pair index's bits, in
+// order, are local bits of the tile other than the Hadamard's.  Lane bits
+// 0-2: local bit K-3+i when it is no control of the chain, else local bit i;
+// lane bits 3-4 and the bit shared by a thread's two butterflies: bits that
+// are no control first; then the rest.
+ChainMap build_chain_map(const FusedPass &pass, const FusedOp &op) {
+	const unsigned K = pass.K, lt = op.lt;
+	uint32_t ctrl = 0;
+	std::vector<std::pair<unsigned, unsigned>> loc;  // (entry, local bit) of the local controls
+	for(unsigned e = 0; e < op.lc; ++e) {
+		const ChainEntry &ce = pass.chain[op.tab + e];
+		if(ce.local >= 0) {
+			ctrl |= 1u << ce.local;
+			loc.push_back({e, (unsigned)ce.local});
+		}
+	}
+	auto is_free = [&](unsigned b) { return b != lt && !((ctrl >> b) & 1u); };
+	uint32_t used = 1u << lt;
+	std::vector<unsigned> order;
+	auto take = [&](unsigned b) {
+		order.push_back(b);
+		used |= 1u << b;
+	};
+	for(unsigned i = 0; i < 3; ++i) {
+		const unsigned hi = K - 3 + i;
+		if(is_free(hi)) take(hi);
+		else if(i != lt) take(i);
+		else take(hi);
+	}
+	auto next = [&](bool want_free) -> int {
+		for(unsigned b = 0; b < K; ++b)
+			if(!((used >> b) & 1u) && (!want_free || is_free(b))) return (int)b;
+		return -1;
+	};
+	for(unsigned i = 3; i < 5; ++i) {
+		int b = next(true);
+		if(b < 0) b = next(false);
+		take((unsigned)b);
+	}
+	const int ilp = next(true);
+	if(ilp >= 0) take((unsigned)ilp);
+	for(int b = next(false); b >= 0; b = next(false)) take((unsigned)b);
+	if(order.size() != K - 1) fail(TMFQS_ERR_LOGIC, "fused pass: chain layout");
+	ChainMap m{};
+	m.nq = 1u << (K - 6);
+	m.ilp = ilp >= 0 ? 1u : 0u;
+	auto mask_of = [&](unsigned j) {
+		uint64_t r = 0;
+		for(const auto &pe : loc)
+			if((j >> pe.second) & 1u) r |= 1ull << (63 - pe.first);
+		return r;
+	};
+	for(unsigned l = 0; l < 32; ++l) {
+		unsigned j = 0;
+		for(unsigned i = 0; i < 5; ++i)
+			if((l >> i) & 1u) j |= 1u << order[i];
+		m.jl[l] = (uint16_t)j;
+		m.ml[l] = mask_of(j);
+	}
+	for(unsigned q = 0; q < m.nq; ++q) {
+		unsigned j = 0;
+		for(unsigned i = 0; 5 + i < K - 1; ++i)
+			if((q >> i) & 1u) j |= 1u << order[5 + i];
+		m.jr[q] = (uint16_t)j;
+		m.mr[q] = mask_of(j);
+	}
+	return m;
+}
+
 template <typename R>
 void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_prog, size_t &dev_prog_bytes) {
 	FusedGeom g{};
@@ -593,9 +798,25 @@ void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	g.ntiles = 1ull << (pass.n - pass.K);
 	g.nops = (unsigned)pass.ops.size();
 	g.inv = 1.0 / std::sqrt(2.0);
-	const size_t ops_bytes = pass.ops.size() * sizeof(FusedOp);
+	// Tiles of >= 7 local bits: swizzled shared memory and per-chain thread layouts.
+	const bool mapped = pass.K >= 7;
+	g.sw = mapped ? pass.K - 3 : 31u;
+	std::vector<FusedOp> ops(pass.ops);
+	std::vector<ChainMap> maps;
+	for(auto &op : ops) {
+		if(op.kind != kFHChain) continue;
+		if(mapped && op.lc <= 64) {
+			op.state = maps.size();
+			maps.push_back(build_chain_map(pass, op));
+		} else {
+			op.state = kNoChainMap;
+		}
+	}
+	const size_t ops_bytes = ops.size() * sizeof(FusedOp);
 	const size_t ph_off = (ops_bytes + 255) & ~size_t(255);
-	const size_t need = ph_off + std::max<size_t>(32, pass.chain.size() * sizeof(ChainEntry));
+	const size_t ch_bytes = std::max<size_t>(32, pass.chain.size() * sizeof(ChainEntry));
+	const size_t map_off = (ph_off + ch_bytes + 255) & ~size_t(255);
+	const size_t need = map_off + std::max<size_t>(32, maps.size() * sizeof(ChainMap));
 	if(need > dev_prog_bytes) {
 		if(dev_prog) {
 			check_cuda(cudaStreamSynchronize(c.stream), "fused program sync");
@@ -611,8 +832,9 @@ void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	}
 	// The program buffer is reused: the upload is ordered on the stream after the pass that read it last.
 	std::vector<unsigned char> host(need, 0);
-	std::memcpy(host.data(), pass.ops.data(), ops_bytes);
+	std::memcpy(host.data(), ops.data(), ops_bytes);
 	if(!pass.chain.empty()) std::memcpy(host.data() + ph_off, pass.chain.data(), pass.chain.size() * sizeof(ChainEntry));
+	if(!maps.empty()) std::memcpy(host.data() + map_off, maps.data(), maps.size() * sizeof(ChainMap));
 	upload_async(c, dev_prog, host.data(), need, "fused program upload");
 	const size_t smem = (sizeof(typename Vec2<R>::type) << pass.K) + (sizeof(uint64_t) << (pass.K - g.m));
 	check_cuda(cudaFuncSetAttribute(k_fused<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fused smem");
@@ -621,7 +843,8 @@ void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	const uint64_t grid = std::min<uint64_t>(g.ntiles, (uint64_t)c.num_sms * std::max(1, per_sm));
 	k_fused<R><<<(unsigned)grid, kFusedThreads, smem, c.stream>>>(
 		static_cast<typename Vec2<R>::type *>(a), g, static_cast<const FusedOp *>(dev_prog),
-		reinterpret_cast<const ChainEntry *>(static_cast<unsigned char *>(dev_prog) + ph_off));
+		reinterpret_cast<const ChainEntry *>(static_cast<unsigned char *>(dev_prog) + ph_off),
+		reinterpret_cast<const ChainMap *>(static_cast<unsigned char *>(dev_prog) + map_off));
 	after_launch(c, "fused pass");
 }
 
