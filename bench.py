@@ -42,9 +42,25 @@ between steps.
           30-qubit complex64 state: the 3xTF32 tensor-core GEMM kernel beside
           the CUDA-core gate kernel, with its HBM fraction and its relative L2
           difference from the CUDA-core result.
+  unmodified_simulator  QFT-28 through the reference's own, unmodified
+          sim::Simulator and QuantumRegister (one backend call per operation)
+          with the integration patch's gpu strategy (tests/dropin), beside the
+          fused path above: the cost of per-operation calls without the
+          batching hooks.
   --impl reference   the reference's own Dense CPU path (oracle/_ref, compiled
-          from the reference sources) on this host, on a bounded prefix of the
-          same circuit.
+          from the reference sources) on this host, on a bounded sample of the
+          same circuit: every 14th operation of QFT-28 (30 operations of all
+          kinds: Hadamards, controlled phases on near and far qubits, swaps),
+          timed by the reference's Simulator.
+
+roofline: the plain form's dominant kernel k_fused<double> is bound by FP64
+instruction issue, not HBM: every controlled phase is its own rounded complex
+product in the reference's operation order (4 DMUL + 2 DADD, no FMA), and a
+Hadamard butterfly is 4 FP64 operations per amplitude.  `achieved` is the
+algorithmic FP64 operations of the passes (4 per amplitude per Hadamard, 1.5
+per amplitude per controlled phase) over their CUDA-event time, against the
+B200's nominal FP64 rate (148 SMs x 64 FP64 lanes x the sampled SM clock);
+the HBM fraction of the same launches is reported beside it.
 
 Multi-GPU: the path does not shard at this tier -- N ranks run N independent
 replicas ("scaling": "weak").
@@ -66,7 +82,9 @@ sys.path.insert(0, ROOT)
 METRIC = "QFT/Grover amp-updates/s, %HBM peak: FP32-fused vs FP64-plain; adjoint grad/s"
 UNIT = "amp-updates/s"
 SEED = 123456
-REF_PREFIX_OPS = 8  # reference CPU sample: H(0) + 7 controlled phases of QFT-28 per step
+REF_SAMPLE_STRIDE = 14  # reference CPU sample: every 14th operation of the QFT circuit
+FP64_LANES_PER_SM = 64  # B200 FP64 pipe: DMUL/DADD per SM per clock (nominal)
+NUM_SMS = 148
 
 
 def parse_args():
@@ -82,7 +100,27 @@ def parse_args():
     p.add_argument("--no-forms", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the QFT-32 and Grover-30 sections")
+    p.add_argument("--no-dropin", action="store_true", help="skip the unmodified-Simulator timing")
     return p.parse_args()
+
+
+def cpu_model():
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            if line.startswith("Model name:"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return None
+
+
+def qft_fp64_ops_per_amp(n):
+    """Algorithmic FP64 operations per amplitude of the exact QFT-n: a Hadamard
+    butterfly is 8 operations per pair (dense_state_backend.cpp:265-271), a
+    controlled phase 6 per amplitude with both bits set (:300-301), a quarter
+    of the state; the swaps move data only."""
+    return 4.0 * n + 1.5 * (n * (n - 1) // 2)
 
 
 def dist_env():
@@ -389,46 +427,104 @@ def run_qft32(tq, torch, device, peak):
     return out
 
 
-def run_grover30(tq, device, peak):
+def run_grover30(tq, torch, device, peak, sweep_iters=64):
+    """Configuration 4: Grover search on 30 qubits, 4 marked states, 12867 iterations.
+
+    Forms: lazy (overlay; O(1) device work per iteration) and materialised,
+    each in complex64 and complex128; the materialised complex128 run in the
+    exact form (all iterations replayed per amplitude in one temporal pass,
+    bit-identical) and in the fast form (the iterations' closed form as one
+    affine sweep, like complex64).  Accuracy of complex64 against complex128:
+    fidelity and relative L2 of the whole logical state, and the marked-state
+    probability error.  The per-iteration sweep form (materialised diffusion
+    as one update sweep per iteration, the cached sum maintained exactly as
+    QuantumRegister does) is timed over `sweep_iters` iterations with its HBM
+    fraction."""
     import math
 
     n, nm = 30, 4
     marked = [int(v) for v in tq.uniform_states(SEED, nm, 0, (1 << n) - 1)]
     iters = int(math.floor(math.pi / 4.0 * math.sqrt((1 << n) / nm)))
     out = {"n_qubits": n, "marked": marked, "iterations": iters}
-    probs = {}
-    for name, prec, b in (("complex64", tq.FP32, 8), ("complex128", tq.FP64, 16)):
+
+    def prepared(prec, exact=True, fusion=True):
         g = tq.GpuState(prec, device)
-        try:
-            for mat in (False, True):
-                g.init_basis(n, 0)
-                g.apply_ops([tq.h(q) for q in range(n)])
-                view = tq.RegisterView.fresh()
-                g.sync()
-                t0 = time.perf_counter()
-                g.grover_run(view, marked, iters, mat)
-                g.sync()
-                secs = time.perf_counter() - t0
-                p = 0.0
-                for s in marked:
-                    re, im = g.amplitude(s)
-                    if view.overlay:
-                        re, im = ((view.scale_re * re - view.scale_im * im) + view.bias_re,
-                                  (view.scale_re * im + view.scale_im * re) + view.bias_im)
-                    p += re * re + im * im
-                form = "materialized" if mat else "lazy"
-                sweep = 2 * b * (1 << n)
-                d = {"seconds": secs, "us_per_iteration": secs / iters * 1e6, "p_marked": p}
-                if mat:
-                    # All iterations in one temporal pass: one sweep instead of one per iteration.
-                    d["sweep_equivalent_frac"] = iters * sweep / secs / 1e9 / peak
-                    d["hbm_frac_actual"] = sweep / secs / 1e9 / peak
-                out[f"{name}_{form}"] = d
-                probs[(name, form)] = p
-        finally:
-            g.close()
+        g.set_option(tq.OPT_EXACT, 1 if exact else 0)
+        g.set_option(tq.OPT_GROVER_FUSION, 1 if fusion else 0)
+        g.init_basis(n, 0)
+        g.apply_ops([tq.h(q) for q in range(n)])
+        return g, tq.RegisterView.fresh()
+
+    def p_marked(g, view):
+        p = 0.0
+        for st in marked:
+            re, im = g.amplitude(st)
+            if view.overlay:
+                re, im = ((view.scale_re * re - view.scale_im * im) + view.bias_re,
+                          (view.scale_re * im + view.scale_im * re) + view.bias_im)
+            p += re * re + im * im
+        return p
+
     for form in ("lazy", "materialized"):
-        out[f"p_marked_err_c64_{form}"] = abs(probs[("complex64", form)] - probs[("complex128", form)])
+        mat = form == "materialized"
+        runs = [("complex64", tq.FP32, True), ("complex128", tq.FP64, True)]
+        if mat:
+            runs.append(("complex128_fast", tq.FP64, False))
+        held = {}
+        for name, prec, exact in runs:
+            g, view = prepared(prec, exact)
+            g.sync()
+            t0 = time.perf_counter()
+            g.grover_run(view, marked, iters, mat)
+            g.sync()
+            secs = time.perf_counter() - t0
+            d = {"seconds": secs, "us_per_iteration": secs / iters * 1e6, "p_marked": p_marked(g, view)}
+            if mat:
+                d["algorithm"] = ("one temporal pass: every iteration replayed per amplitude in registers, bit-identical"
+                                  if exact and prec == tq.FP64 else
+                                  "closed form: K iterations as one affine sweep (FP64 scalars, rounded once)")
+            out[f"{name}_{form}"] = d
+            if view.overlay:  # materialise the overlay so the stored state is the logical one
+                g.affine((view.scale_re, view.scale_im), (view.bias_re, view.bias_im))
+            if name == "complex128_fast":
+                g.close()
+            else:
+                held[name] = g
+        fid, rel = _compare(torch, held["complex128"].tensor(), held["complex64"].tensor())
+        out[f"fidelity_c64_vs_c128_{form}"] = fid
+        out[f"rel_l2_c64_vs_c128_{form}"] = rel
+        out[f"p_marked_err_c64_{form}"] = abs(out[f"complex64_{form}"]["p_marked"] - out[f"complex128_{form}"]["p_marked"])
+        for g in held.values():
+            g.close()
+        torch.cuda.empty_cache()
+    m = out
+    m["speedup_c64_vs_c128_exact_materialized"] = m["complex128_materialized"]["seconds"] / m["complex64_materialized"]["seconds"]
+    m["speedup_c64_vs_c128_fast_materialized"] = (m["complex128_fast_materialized"]["seconds"] /
+                                                  m["complex64_materialized"]["seconds"])
+    m["speedup_c64_vs_c128_lazy"] = m["complex128_lazy"]["seconds"] / m["complex64_lazy"]["seconds"]
+
+    # The per-iteration sweep form: one inversion sweep per iteration.
+    for name, prec, b in (("complex64", tq.FP32, 8), ("complex128", tq.FP64, 16)):
+        g, view = prepared(prec, True, fusion=False)
+        g.grover_run(view, marked, 2, True)  # warm-up: the first sum pass and the first sweeps
+        g.sync()
+        g.reset_stats()
+        g.set_option(tq.OPT_KERNEL_TIMING, 1)
+        t0 = time.perf_counter()
+        g.grover_run(view, marked, sweep_iters, True)
+        g.sync()
+        secs = time.perf_counter() - t0
+        kt = g.kernel_times()
+        g.set_option(tq.OPT_KERNEL_TIMING, 0)
+        g.close()
+        sweep = 2 * b * (1 << n)
+        gate = kt["gate"]
+        dev_ms = gate["ms"] / max(1, gate["launches"])
+        out[f"{name}_per_iteration_sweep"] = {
+            "iterations_timed": sweep_iters, "ms_per_iteration": secs / sweep_iters * 1e3,
+            "sweep_ms": dev_ms, "sweeps": gate["launches"], "bytes_per_sweep": sweep,
+            "hbm_frac": sweep / (dev_ms / 1e3) / 1e9 / peak if gate["launches"] else None,
+            "projected_seconds_all_iterations": secs / sweep_iters * iters}
     return out
 
 
@@ -457,6 +553,25 @@ def run_block_gate(tq, torch, device, peak, reps=3):
     for g in states.values():
         g.close()
     return out
+
+
+def run_unmodified_simulator(n, fused_ms):
+    """QFT-n through the reference's own Simulator/QuantumRegister on the gpu
+    strategy (tests/dropin, integration patch only): one backend call, and so
+    one device pass, per operation."""
+    exe = os.path.join(ROOT, "tests", "dropin", "_build", "bin", "qft_through_simulator")
+    if not os.path.exists(exe):
+        return {"unavailable": "tests/dropin not built"}
+    env = dict(os.environ)
+    env["LD_LIBRARY_PATH"] = os.path.join(ROOT, "tmfqsfullstate_b200") + ":" + env.get("LD_LIBRARY_PATH", "")
+    p = subprocess.run([exe, str(n), "gpu", str(SEED)], capture_output=True, text=True, timeout=900, env=env)
+    if p.returncode != 0:
+        return {"unavailable": (p.stdout + p.stderr)[-300:]}
+    r = json.loads(p.stdout.strip().splitlines()[-1])
+    r["execution_over_fused_step"] = r["execution_seconds"] * 1e3 / fused_ms
+    r["note"] = ("Simulator executionSeconds: the circuit's operations one backend call each (no batching hooks); "
+                 "run_wall_seconds adds the 4 GiB input load and the export of the result into a host QuantumState")
+    return r
 
 
 def run_ours(args):
@@ -531,6 +646,23 @@ def run_ours(args):
         t1 = time.perf_counter()
         e2e_times.append(t1 - t0)
     e2e_s = statistics.median(e2e_times)
+    # The whole output state against the reference's own (tests/golden/qft28_ref.json: SHA-256 of the
+    # reference Dense backend's 4 GiB result, its argmax): bit for bit, so relL2 = 0.
+    whole_state = None
+    gold_path = os.path.join(ROOT, "tests", "golden", f"qft{n}_ref.json")
+    if rank == 0 and os.path.exists(gold_path):
+        import hashlib
+
+        with open(gold_path) as fh:
+            gold = json.load(fh)
+        out_state = g.export()
+        digest = hashlib.sha256(memoryview(out_state).cast("B")).hexdigest()
+        prob = out_state[0::2] * out_state[0::2] + out_state[1::2] * out_state[1::2]
+        arg = int(np.argmax(prob))
+        whole_state = {"sha256_equals_reference": digest == gold["sha256"], "argmax": arg,
+                       "argmax_equals_reference": arg == gold["argmax"],
+                       "rel_l2_vs_reference": 0.0 if digest == gold["sha256"] else None}
+        del out_state, prob
     if world > 1:
         t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -543,10 +675,21 @@ def run_ours(args):
     if fused["launches"]:
         bytes_per = fused["bytes"] / fused["launches"]
         avg_ms = fused["ms"] / fused["launches"]
-        achieved = bytes_per / (avg_ms / 1e3) / 1e9
-        roofline = {"bound": "hbm", "kernel": "k_fused<double> (fused multi-gate pass)", "achieved": achieved,
-                    "peak": peak, "peak_source": f"{peak_kind} hbm_gbs", "unit": "GB/s", "frac": achieved / peak,
+        hbm = bytes_per / (avg_ms / 1e3) / 1e9
+        # FP64 operations of the fused passes per launch (each QFT step's fused passes hold all its H and CP).
+        launches_per_step = fused["launches"] / args.steps
+        fp64_per_launch = qft_fp64_ops_per_amp(n) * N / launches_per_step
+        sm_mhz = clk.get("sm_mhz") or 1965.0
+        fp64_peak = NUM_SMS * FP64_LANES_PER_SM * sm_mhz * 1e6 / 1e12
+        achieved = fp64_per_launch / (avg_ms / 1e3) / 1e12
+        roofline = {"bound": "fp64", "kernel": "k_fused<double> (fused multi-gate pass, exact)", "achieved": achieved,
+                    "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                    "peak_source": f"nominal FP64 issue rate: {NUM_SMS} SMs x {FP64_LANES_PER_SM} lanes x {sm_mhz:.0f} MHz "
+                                   f"(median SM clock sampled in the timed region)",
+                    "fp64_ops_per_launch": fp64_per_launch, "fp64_ops_per_amplitude_qft": qft_fp64_ops_per_amp(n),
                     "traffic": profiled_traffic(n), "bytes_per_launch": bytes_per, "avg_launch_ms": avg_ms,
+                    "hbm": {"achieved": hbm, "peak": peak, "unit": "GB/s", "frac": hbm / peak,
+                            "peak_source": f"{peak_kind} hbm_gbs"},
                     "share_of_step": fused["ms"] / ms if ms else None}
 
     forms = None
@@ -565,8 +708,12 @@ def run_ours(args):
         adjoint = run_adjoint(tq, torch, local)
     configs = None
     if rank == 0 and not args.no_configs:
-        configs = {"qft32": run_qft32(tq, torch, local, peak), "grover30": run_grover30(tq, local, peak),
+        configs = {"qft32": run_qft32(tq, torch, local, peak), "grover30": run_grover30(tq, torch, local, peak),
                    "block_gate": run_block_gate(tq, torch, local, peak)}
+
+    dropin = None
+    if rank == 0 and not args.no_dropin:
+        dropin = run_unmodified_simulator(n, ms_per_step)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -583,9 +730,9 @@ def run_ours(args):
                     "ms_per_step": e2e_s * 1e3},
             "gpu_launches": int(stats["kernel_launches"]),
             "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "forms": forms,
-            "adjoint": adjoint, "configs": configs,
+            "adjoint": adjoint, "configs": configs, "unmodified_simulator": dropin,
             "kernel_times_ms": {k: round(v["ms"], 3) for k, v in kt.items() if v["launches"]},
-            "check": {"total_probability": total, "measured": measured,
+            "check": {"total_probability": total, "measured": measured, "whole_state": whole_state,
                       "reference_golden": {"total_probability": 0.99999999999986022, "measured": 138222191}},
         }
         print(json.dumps(out), flush=True)
@@ -594,36 +741,48 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def reference_sample(n, prefix_ops, steps, warmup):
-    """The reference Dense CPU path (oracle/_ref) on the first `prefix_ops` ops of QFT-n."""
+def reference_sample(n, stride, steps, warmup, per_step=None):
+    """The reference Dense CPU path (oracle/_ref) on every `stride`-th op of QFT-n
+    (all kinds of the circuit's operations, in circuit order).  With per_step,
+    each step runs the next `per_step` ops of that sample (cycling), so that
+    many steps stay within minutes.  Returns (kind, seconds per timed step,
+    ops per timed step)."""
     import oracle as O
 
     src = "reference" if O.ref_available() else "port"
-    ops = (O.ref_qft_ops(n) if src == "reference" else O.qft_ops(n))[:prefix_ops]
-    secs = []
+    sample = (O.ref_qft_ops(n) if src == "reference" else O.qft_ops(n))[::stride]
+    k = per_step or len(sample)
+    chunks = [[sample[(i * k + j) % len(sample)] for j in range(k)] for i in range(warmup + steps)]
+    secs, nops = [], []
     if src == "reference":
         st = O.RefState(n, "random_phase", seed=SEED)
-        for i in range(warmup + steps):
+        for i, ops in enumerate(chunks):
             r = st.run(ops, want_amps=False)
             if i >= warmup:
                 secs.append(r["seconds"])
+                nops.append(len(ops))
     else:
         amps = O.random_phase(n, SEED)
-        for i in range(warmup + steps):
+        for i, ops in enumerate(chunks):
             reg = O.OracleRegister(n, amps=amps)
             t0 = time.perf_counter()
             reg.run(ops)
             if i >= warmup:
                 secs.append(time.perf_counter() - t0)
-    return src, secs, len(ops)
+                nops.append(len(ops))
+    return src, secs, nops
+
+
+def sample_text(n, nops):
+    return (f"every {REF_SAMPLE_STRIDE}th operation of QFT-{n} ({nops} ops: Hadamards, controlled phases, swaps) "
+            f"on the random-phase input, reference Simulator executionSeconds, single-threaded Dense backend")
 
 
 def cpu_baseline(n):
-    src, secs, nops = reference_sample(n, REF_PREFIX_OPS, 1, 0)
-    v = nops * (1 << n) / statistics.median(secs)
-    return {"value": v, "unit": UNIT, "cores": 1, "kind": src,
-            "sample": f"first {nops} ops of QFT-{n} (H(0) + controlled phases) on the random-phase input, "
-                      f"reference Simulator executionSeconds, single-threaded Dense backend"}
+    src, secs, nops = reference_sample(n, REF_SAMPLE_STRIDE, 1, 0)
+    v = sum(nops) * (1 << n) / sum(secs)
+    return {"value": v, "unit": UNIT, "cores": 1, "kind": src, "cpu_model": cpu_model(), "host_threads": os.cpu_count(),
+            "sample": sample_text(n, sum(nops))}
 
 
 def run_reference(args):
@@ -631,16 +790,17 @@ def run_reference(args):
     if rank != 0:
         return
     n = args.qubits
+    per_step = 5
     try:
-        src, secs, nops = reference_sample(n, REF_PREFIX_OPS, args.steps, args.warmup)
+        src, secs, nops = reference_sample(n, REF_SAMPLE_STRIDE, args.steps, args.warmup, per_step)
     except Exception as e:  # the reference could not run here
         print(json.dumps({"impl": "reference", "unavailable": f"{type(e).__name__}: {e}"}))
         return
-    s = statistics.median(secs)
-    value = nops * (1 << n) / s
-    cpu = {"value": value, "unit": UNIT, "cores": 1, "kind": src,
-           "sample": f"first {nops} ops of QFT-{n} per step on the random-phase input (reference Dense backend, "
-                     f"one thread; Simulator executionSeconds)"}
+    s = sum(secs) / len(secs)
+    value = sum(nops) * (1 << n) / sum(secs)
+    cpu = {"value": value, "unit": UNIT, "cores": 1, "kind": src, "cpu_model": cpu_model(), "host_threads": os.cpu_count(),
+           "sample": f"{per_step} consecutive ops per step of the sample: " + sample_text(n, per_step * len(secs)) +
+                     " (the Dense backend is single-threaded, so one core)"}
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": s * 1e3, "higher_is_better": True, "scaling": "weak",

@@ -159,6 +159,13 @@ TMFQS_API int tmfqs_gpu_destroy(tmfqs_gpu_state *h);
 /* Deep copy: IStateBackend::clone, storage/i_state_backend.h:31. */
 TMFQS_API int tmfqs_gpu_clone(tmfqs_gpu_state *h, tmfqs_gpu_state **out);
 TMFQS_API const char *tmfqs_gpu_last_error(void);
+/* Test hook, no counterpart in the reference: after `skip` further device
+ * allocations of the library (state, staging, reduction scratch, pass
+ * programs) succeed, the next `count` fail as if cudaMalloc had run out of
+ * memory -- the call then returns TMFQS_ERR_NOMEM, which the C++ binding maps
+ * to std::runtime_error like the reference's other resource failures.  No
+ * device memory is touched.  (0, 0) disarms it.  Process-wide. */
+TMFQS_API int tmfqs_debug_fail_allocations(unsigned skip, unsigned count);
 
 /* ---- initialisation / IO (storage/i_state_backend.h:37-66) ------------ */
 /* initZero, i_state_backend.h:37; dense_state_backend.cpp:77-81. */

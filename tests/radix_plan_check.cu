@@ -13,6 +13,7 @@ namespace tqb {
 	std::exit(2);
 }
 void check_cuda(cudaError_t, const char *) {}
+cudaError_t device_alloc(void **, size_t) { return cudaErrorMemoryAllocation; }
 void upload_async(const LaunchCtx &, void *, const void *, size_t, const char *) {}
 }  // namespace tqb
 

@@ -180,6 +180,7 @@ SIGNATURES = {
     "tmfqs_gpu_stream": [_H, ctypes.POINTER(ctypes.c_void_p)],
     "tmfqs_random_phase": [_UI, ctypes.c_uint32, _DP],
     "tmfqs_sample_static": [ctypes.c_void_p, ctypes.c_int, _UI, _D, ctypes.c_void_p, _U64P],
+    "tmfqs_debug_fail_allocations": [_UI, _UI],
     "tmfqs_mt19937_unit": [ctypes.c_uint32, _U64, _DP],
     "tmfqs_uniform_states": [_U64, _U64, _U64, _U64, _U64P],
 }
@@ -330,6 +331,12 @@ def sample_static(device_amps: int, precision: int, num_qubits: int, rnd: float,
     _check(lib().tmfqs_sample_static(ctypes.c_void_p(device_amps), precision, num_qubits, rnd,
                                      ctypes.c_void_p(stream) if stream else None, ctypes.byref(out)))
     return out.value
+
+
+def debug_fail_allocations(skip: int, count: int) -> None:
+    """Test hook: after `skip` more device allocations succeed, the next `count`
+    fail as out of memory (no device memory is touched); (0, 0) disarms."""
+    _check(lib().tmfqs_debug_fail_allocations(skip, count))
 
 
 def op_array(ops):

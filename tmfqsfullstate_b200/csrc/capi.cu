@@ -8,6 +8,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -24,6 +25,33 @@ void check_cuda(cudaError_t e, const char *what) {
 		cudaGetLastError();
 		throw Error{TMFQS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 	}
+}
+
+namespace {
+std::mutex g_fail_mutex;
+unsigned g_fail_skip = 0, g_fail_count = 0;
+}  // namespace
+
+void arm_alloc_failures(unsigned skip, unsigned count) {
+	std::lock_guard<std::mutex> lock(g_fail_mutex);
+	g_fail_skip = skip;
+	g_fail_count = count;
+}
+
+cudaError_t device_alloc(void **p, size_t bytes) {
+	{
+		std::lock_guard<std::mutex> lock(g_fail_mutex);
+		if(g_fail_count > 0) {
+			if(g_fail_skip > 0) {
+				--g_fail_skip;
+			} else {
+				--g_fail_count;
+				*p = nullptr;
+				return cudaErrorMemoryAllocation;
+			}
+		}
+	}
+	return cudaMalloc(p, bytes);
 }
 
 }  // namespace tqb
@@ -157,7 +185,7 @@ void ensure_state(tmfqs_gpu_state *h, unsigned n) {
 		h->bytes = 0;
 	}
 	tqb::seq_scratch_free(h->seq);
-	if(cudaMalloc(&h->amps, bytes) != cudaSuccess) {
+	if(tqb::device_alloc(&h->amps, bytes) != cudaSuccess) {
 		cudaGetLastError();
 		h->amps = nullptr;
 		h->initialized = false;
@@ -177,7 +205,7 @@ void ensure_dev_small(tmfqs_gpu_state *h, size_t bytes) {
 	h->dev_small = nullptr;
 	h->dev_small_bytes = 0;
 	const size_t sz = std::max<size_t>(bytes, 1 << 16);
-	if(cudaMalloc(&h->dev_small, sz) != cudaSuccess) {
+	if(tqb::device_alloc(&h->dev_small, sz) != cudaSuccess) {
 		cudaGetLastError();
 		fail(TMFQS_ERR_NOMEM, "device staging allocation failed");
 	}
@@ -1205,7 +1233,7 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 		if(h->adj_ckpt) cudaFree(h->adj_ckpt);
 		h->adj_ckpt = nullptr;
 		h->adj_ckpt_bytes = 0;
-		if(cudaMalloc(&h->adj_ckpt, nseg * bytes) != cudaSuccess) {
+		if(tqb::device_alloc((void **)&h->adj_ckpt, nseg * bytes) != cudaSuccess) {
 			cudaGetLastError();
 			h->adj_ckpt = nullptr;
 			fail(TMFQS_ERR_NOMEM, "adjoint gradient: checkpoint allocation failed (raise checkpoint_every)");
@@ -1216,7 +1244,7 @@ void adjoint_gradient(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, con
 	// reduced sums.
 	const size_t chunk = (size_t)tqb::adjoint_max_blocks(h->num_sms) * tqb::kMaxDiagRun;
 	if(!h->adj_part &&
-	   cudaMalloc(&h->adj_part, (chunk * tqb::kMaxPendingSums + tqb::kMaxPendingSums * tqb::kMaxDiagRun) * sizeof(double)) !=
+	   tqb::device_alloc((void **)&h->adj_part, (chunk * tqb::kMaxPendingSums + tqb::kMaxPendingSums * tqb::kMaxDiagRun) * sizeof(double)) !=
 	       cudaSuccess) {
 		cudaGetLastError();
 		h->adj_part = nullptr;
@@ -1782,6 +1810,11 @@ int tmfqs_gpu_gate(tmfqs_gpu_state *h, const double *matrix, const unsigned *qub
 		before_mutation(h);
 		run_gate(h, matrix, qubits, k);
 	});
+}
+
+int tmfqs_debug_fail_allocations(unsigned skip, unsigned count) {
+	tqb::arm_alloc_failures(skip, count);
+	return TMFQS_OK;
 }
 
 int tmfqs_gpu_apply_ops(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count) {

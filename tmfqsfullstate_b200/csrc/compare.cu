@@ -80,7 +80,7 @@ void launch_compare(const LaunchCtx &c, int prec_ref, const void *ref, int prec_
                     CompareReport &out) {
 	const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((N + kCmpThreads - 1) / kCmpThreads, (uint64_t)c.num_sms * 4));
 	CmpPartial *dev = nullptr;
-	if(cudaMalloc(&dev, sizeof(CmpPartial) * blocks) != cudaSuccess) {
+	if(device_alloc((void **)&dev, sizeof(CmpPartial) * blocks) != cudaSuccess) {
 		cudaGetLastError();
 		fail(TMFQS_ERR_NOMEM, "compare: scratch allocation failed");
 	}

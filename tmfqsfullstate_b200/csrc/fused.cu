@@ -824,7 +824,7 @@ void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 		}
 		dev_prog = nullptr;
 		dev_prog_bytes = 0;
-		if(cudaMalloc(&dev_prog, need * 2) != cudaSuccess) {
+		if(device_alloc(&dev_prog, need * 2) != cudaSuccess) {
 			cudaGetLastError();
 			fail(TMFQS_ERR_NOMEM, "fused pass program allocation failed");
 		}

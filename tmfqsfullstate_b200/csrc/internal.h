@@ -25,6 +25,13 @@ struct Error {
 [[noreturn]] void fail(int status, const std::string &message);
 void check_cuda(cudaError_t e, const char *what);
 
+// cudaMalloc for the library's device buffers.  While the failure knob of
+// tmfqs_debug_fail_allocations is armed it returns cudaErrorMemoryAllocation
+// instead (without calling cudaMalloc), so the out-of-memory paths can be
+// tested on the host side without exhausting a GPU.
+cudaError_t device_alloc(void **p, size_t bytes);
+void arm_alloc_failures(unsigned skip, unsigned count);
+
 // ---------------------------------------------------------------------------
 // Exact sequential-sum engine (seqsum.cu)
 // ---------------------------------------------------------------------------

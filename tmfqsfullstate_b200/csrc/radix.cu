@@ -863,7 +863,7 @@ bool run_radix(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 		dev_prog = nullptr;
 		dev_prog_bytes = 0;
 		const size_t want = need + need / 8;
-		if(cudaMalloc(&dev_prog, want) != cudaSuccess) {
+		if(device_alloc((void **)&dev_prog, want) != cudaSuccess) {
 			cudaGetLastError();
 			fail(TMFQS_ERR_NOMEM, "radix pass program allocation failed");
 		}

@@ -554,7 +554,7 @@ void ensure_scratch(SeqScratch &s, uint64_t N) {
 	             b_wo = align(sizeof(WalkOut));
 	const size_t total = b_ta + b_tp + b_tb + b_ga + b_gp + b_gb + b_wo;
 	void *base = nullptr;
-	if(cudaMalloc(&base, total) != cudaSuccess) {
+	if(device_alloc(&base, total) != cudaSuccess) {
 		cudaGetLastError();
 		fail(TMFQS_ERR_NOMEM, "exact reduction scratch: device allocation of " + std::to_string(total) + " bytes failed");
 	}

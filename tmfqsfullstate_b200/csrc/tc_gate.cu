@@ -252,7 +252,7 @@ void launch_tc_gate(const LaunchCtx &c, void *a, unsigned n, unsigned k, const d
 		}
 		dev_buf = nullptr;
 		dev_buf_bytes = 0;
-		if(cudaMalloc(&dev_buf, need) != cudaSuccess) {
+		if(device_alloc((void **)&dev_buf, need) != cudaSuccess) {
 			cudaGetLastError();
 			fail(TMFQS_ERR_NOMEM, "tensor-core gate: allocation failed");
 		}

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "tmfqsfs.h"
+#include "tmfqs_b200.h"
 
 using namespace tmfqs;
 
@@ -256,6 +257,33 @@ void operationsAndSwaps() {
 
 }  // namespace
 
+// The C-ABI status classes through GpuStateBackend's exception mapping:
+// out_of_range, invalid_argument, logic_error (an uninitialised backend) and
+// runtime_error for device out-of-memory, injected on the host with
+// tmfqs_debug_fail_allocations (no device memory is exhausted).
+void failureMapping() {
+	RegisterConfig cfg;
+	cfg.strategy = StorageStrategyKind::Gpu;
+	std::unique_ptr<IStateBackend> raw = StateBackendFactory::create(4, cfg);
+	REQUIRE(throwsAs<std::logic_error>([&] { raw->applyHadamard(0); }));
+	REQUIRE(throwsAs<std::logic_error>([&] { (void)raw->totalProbability(); }));
+	raw->initZero(4);
+	REQUIRE(throwsAs<std::out_of_range>([&] { raw->applyHadamard(4); }));
+	REQUIRE(throwsAs<std::invalid_argument>([&] { raw->applyControlledNot(1, 1); }));
+	REQUIRE(throwsAs<std::invalid_argument>([&] { (void)raw->sampleMeasurement(1.0); }));
+
+	tmfqs_debug_fail_allocations(0, 1);
+	REQUIRE(throwsAs<std::runtime_error>([&] { QuantumRegister q(20, 0); }));
+	QuantumRegister ok(20, 0);  // the knob fired once; allocation works again
+	ok.applyHadamard(3);
+	tmfqs_debug_fail_allocations(0, 1);
+	REQUIRE(throwsAs<std::runtime_error>([&] { QuantumRegister copy(ok); }));
+	tmfqs_debug_fail_allocations(0, 0);
+	QuantumRegister copy(ok);
+	REQUIRE(copy.amplitude(0).real == ok.amplitude(0).real);
+	REQUIRE(std::fabs(copy.totalProbability() - 1.0) < 1e-12);
+}
+
 int main() {
 	try {
 		qftKnownAnswers();
@@ -265,6 +293,7 @@ int main() {
 		registryAndCopies();
 		batchedEqualsPerOperation();
 		operationsAndSwaps();
+		failureMapping();
 	} catch(const std::exception &e) {
 		std::cout << "FAILED after " << g_checks << " checks: " << e.what() << "\n";
 		return 1;
