@@ -314,6 +314,27 @@ TMFQS_API int tmfqs_gpu_set_option(tmfqs_gpu_state *h, int option, long value);
  * (synchronises the stream; `out` has TMFQS_KT_COUNT entries).  Reset with
  * tmfqs_gpu_reset_stats. */
 TMFQS_API int tmfqs_gpu_kernel_times(tmfqs_gpu_state *h, tmfqs_kernel_time *out);
+/* One timed device pass (recorded while TMFQS_OPT_KERNEL_TIMING is on).  The
+ * per-operation trace of sim::Simulator (simulator.cpp:72-82, RunReport of
+ * report.cpp:39-93) becomes one entry per pass when operations are fused:
+ * a pass of tmfqs_gpu_apply_ops covers ops [first_op, first_op + op_count) of
+ * that call; other launches (Grover runs, reductions) have op_count 0. */
+typedef struct tmfqs_pass_record {
+	int kind;          /* TMFQS_KT_* class */
+	unsigned op_count; /* operations of the apply_ops call the pass applied (0: not a gate batch) */
+	uint64_t segment;  /* the handle's segment number when the pass was launched (tmfqs_gpu_pass_mark) */
+	uint64_t first_op; /* index of its first operation within that tmfqs_gpu_apply_ops call */
+	double ms;         /* CUDA-event time on the handle's stream */
+	double bytes;      /* algorithmic HBM bytes of the pass */
+} tmfqs_pass_record;
+/* Starts a new segment of the pass log and returns its number (segments let a
+ * caller map passes back to the calls it made).  tmfqs_gpu_reset_stats clears
+ * the log and restarts the numbering at 0. */
+TMFQS_API int tmfqs_gpu_pass_mark(tmfqs_gpu_state *h, uint64_t *segment_out);
+/* Waits for the handle's stream, then copies up to `capacity` records of the
+ * log (oldest first) and sets *count to the log's length (out may be NULL to
+ * query it). */
+TMFQS_API int tmfqs_gpu_pass_log(tmfqs_gpu_state *h, tmfqs_pass_record *out, size_t capacity, size_t *count);
 /* The handle's device buffer and CUDA stream (for device-resident benchmarks
  * and interop; the buffer stays owned by the handle). */
 TMFQS_API int tmfqs_gpu_device_buffer(tmfqs_gpu_state *h, void **ptr, size_t *bytes);

@@ -29,7 +29,7 @@ def test_state_allocation_failure_is_reported_and_recoverable():
             g.init_zero(20)
         with pytest.raises(tq.LogicError):
             g.total_probability()  # nothing was initialised
-        g.init_zero(20)
+        g.init_basis(20, 0)
         assert g.total_probability() == 1.0
 
 

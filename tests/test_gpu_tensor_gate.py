@@ -91,9 +91,13 @@ def test_dense_block_fusion(window):
     r.run(theirs)
     want = r.amplitudes()
     outs, passes = [], []
-    for tensor in (1, 0):
-        with tq.GpuState(tq.FP32) as g:
+    # complex64 on the tensor cores, complex64 on the CUDA-core block kernel,
+    # the fast complex128 form (CUDA-core blocks), the exact complex128 form
+    # (no blocks: gate by gate, bit-identical).
+    for prec, tensor, exact in ((tq.FP32, 1, 1), (tq.FP32, 0, 1), (tq.FP64, 1, 0), (tq.FP64, 1, 1)):
+        with tq.GpuState(prec) as g:
             g.set_option(tq.OPT_TENSOR, tensor)
+            g.set_option(tq.OPT_EXACT, exact)
             g.load(n, a)
             g.reset_stats()
             g.apply_ops(ours)
@@ -102,6 +106,35 @@ def test_dense_block_fusion(window):
             outs.append(g.export())
     assert O.rel_l2(want, outs[0]) < 1e-5
     assert O.rel_l2(outs[1], outs[0]) < 1e-5
+    assert O.rel_l2(want, outs[2]) < 1e-12
+    assert np.array_equal(want, outs[3])
     if len(window) <= 5:
-        assert passes[0] == 1  # the whole circuit is one block
-    assert passes[0] < passes[1]
+        assert passes[0] == passes[2] == 1  # the whole circuit is one block
+    assert passes[0] == passes[1] == passes[2] < passes[3]
+
+
+@pytest.mark.parametrize("prec,exact,tol", [(tq.FP32, 1, 1e-5), (tq.FP64, 0, 1e-12)])
+def test_block_that_starts_with_gates_before_the_dense_gate(prec, exact, tol):
+    """H, a controlled phase and a CNOT that lead into a dense gate, and the
+    gates after it, within five qubits, make one block: one sweep for the run
+    (fast forms)."""
+    n = 18
+    u = unitary(4, 11)
+    ours = [tq.h(2), tq.cphase(2, 5, 0.7), tq.cnot(5, 9), tq.gate(u, np.array([5, 9], dtype=np.uint32)), tq.x(9),
+            tq.h(0), tq.h(1)]
+    theirs = [O.h(2), O.cphase(2, 5, 0.7), O.cnot(5, 9), O.gate(u, [5, 9]), O.x(9), O.h(0), O.h(1)]
+    rng = np.random.default_rng(5)
+    a = rng.standard_normal(2 << n)
+    a /= np.linalg.norm(a)
+    r = O.OracleRegister(n, amps=a)
+    r.run(theirs)
+    with tq.GpuState(prec) as g:
+        g.set_option(tq.OPT_EXACT, exact)
+        g.load(n, a)
+        g.reset_stats()
+        g.apply_ops(ours)
+        st = g.stats()
+        got = g.export()
+    assert O.rel_l2(r.amplitudes(), got) < tol
+    # All seven ops act within qubits {2, 5, 9, 0, 1}: one block sweep, no other pass.
+    assert st["gate_passes"] == 1 and st["fused_passes"] == 0

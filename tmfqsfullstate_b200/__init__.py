@@ -108,6 +108,13 @@ OPT_TENSOR = 6
 OPT_QFT_PASS = 7
 
 
+class PassRecord(ctypes.Structure):
+    """tmfqs_pass_record: one timed device pass."""
+
+    _fields_ = [("kind", ctypes.c_int), ("op_count", ctypes.c_uint), ("segment", ctypes.c_uint64),
+                ("first_op", ctypes.c_uint64), ("ms", ctypes.c_double), ("bytes", ctypes.c_double)]
+
+
 class StateComparison(ctypes.Structure):
     _fields_ = [("bitwise_equal", ctypes.c_int), ("max_abs_amplitude_error", ctypes.c_double),
                 ("max_abs_component_error", ctypes.c_double), ("rmse_amplitude", ctypes.c_double),
@@ -181,6 +188,8 @@ SIGNATURES = {
     "tmfqs_random_phase": [_UI, ctypes.c_uint32, _DP],
     "tmfqs_sample_static": [ctypes.c_void_p, ctypes.c_int, _UI, _D, ctypes.c_void_p, _U64P],
     "tmfqs_debug_fail_allocations": [_UI, _UI],
+    "tmfqs_gpu_pass_mark": [_H, _U64P],
+    "tmfqs_gpu_pass_log": [_H, ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)],
     "tmfqs_mt19937_unit": [ctypes.c_uint32, _U64, _DP],
     "tmfqs_uniform_states": [_U64, _U64, _U64, _U64, _U64P],
 }
@@ -563,6 +572,20 @@ class GpuState:
         arr = (KernelTime * len(KT_NAMES))()
         _check(lib().tmfqs_gpu_kernel_times(self._h, arr))
         return {n: {"launches": arr[i].launches, "ms": arr[i].ms, "bytes": arr[i].bytes} for i, n in enumerate(KT_NAMES)}
+
+    def pass_mark(self) -> int:
+        seg = ctypes.c_uint64()
+        _check(lib().tmfqs_gpu_pass_mark(self._h, ctypes.byref(seg)))
+        return seg.value
+
+    def pass_log(self) -> list:
+        """Timed passes since reset_stats (needs OPT_KERNEL_TIMING on while they ran)."""
+        n = ctypes.c_size_t()
+        _check(lib().tmfqs_gpu_pass_log(self._h, None, 0, ctypes.byref(n)))
+        arr = (PassRecord * max(1, n.value))()
+        _check(lib().tmfqs_gpu_pass_log(self._h, ctypes.cast(arr, ctypes.c_void_p), n.value, ctypes.byref(n)))
+        return [{"kind": KT_NAMES[r.kind], "op_count": r.op_count, "segment": r.segment, "first_op": r.first_op,
+                 "ms": r.ms, "bytes": r.bytes} for r in arr[:n.value]]
 
     def device_buffer(self):
         p, n = ctypes.c_void_p(), ctypes.c_size_t()

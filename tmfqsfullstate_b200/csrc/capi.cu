@@ -114,7 +114,7 @@ class PassTimer {
 		~PassTimer() {
 			if(!h_->opt_timing || !start_) return;
 			if(cudaEventRecord(stop_, h_->stream) == cudaSuccess) {
-				h_->timed.push_back({kind_, start_, stop_, bytes_});
+				h_->timed.push_back({kind_, start_, stop_, bytes_, h_->segment, h_->cur_first, h_->cur_count});
 			} else {
 				cudaGetLastError();
 				cudaEventDestroy(start_);
@@ -138,6 +138,8 @@ void resolve_timers(tmfqs_gpu_state *h) {
 		h->times[t.kind].launches += 1;
 		h->times[t.kind].ms += ms;
 		h->times[t.kind].bytes += t.bytes;
+		if(h->pass_log.size() < (size_t(1) << 22))
+			h->pass_log.push_back(tmfqs_pass_record{t.kind, t.count, t.segment, t.first, (double)ms, t.bytes});
 		cudaEventDestroy(t.start);
 		cudaEventDestroy(t.stop);
 	}
@@ -345,6 +347,7 @@ struct Planner {
 	size_t npass = 0;              // multi-op passes run so far
 	void *mirror = nullptr;        // a radix pass launched by the next flush also writes its result here
 	bool mirrored = false;         // ... and did
+	const tmfqs_op *base = nullptr;  // the apply_ops call's op array (pass-log op indexes)
 
 	explicit Planner(tmfqs_gpu_state *hh) : h(hh) {
 		// Tiles of 2^12 complex128 / 2^13 complex64 amplitudes (64 KB).  The
@@ -440,6 +443,10 @@ struct Planner {
 	// local indices once the local set is known.
 	void flush() {
 		if(pending.empty()) return;
+		if(base) {
+			h->cur_first = (uint64_t)(pending.front() - base);
+			h->cur_count = (unsigned)pending.size();
+		}
 		if(pending.size() == 1) {
 			run_single(*pending[0]);
 		} else {
@@ -920,32 +927,62 @@ bool op_as_matrix(const tmfqs_op &op, std::vector<unsigned> &qs, std::vector<std
 	}
 }
 
-// Starting at ops[i] (a dense gate), the longest run of ops acting within 5
-// qubits, multiplied in FP64 into one block matrix and applied as one
-// tensor-core gate.  Returns the number of ops consumed (0: no block).
-size_t run_dense_block(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t i, size_t count) {
-	typedef std::complex<double> C;
-	std::vector<unsigned> Q;  // block qubits, block order (first = most significant)
-	std::vector<std::pair<std::vector<unsigned>, std::vector<C>>> parts;
+// Block fusion applies to the fast forms only: the block is multiplied out in
+// FP64, which rounds differently from the reference's gate-by-gate products.
+bool block_fusion(const tmfqs_gpu_state *h) { return h->precision == TMFQS_FP32 || !h->opt_exact; }
+
+// The run of ops starting at ops[i] that acts within 5 qubits and that a
+// block can take: its end (exclusive), and whether it holds a dense gate
+// (MatrixGate) -- runs without one are left to the fused passes.
+size_t dense_block_extent(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t i, size_t count, bool &has_gate) {
+	std::vector<unsigned> Q;
+	has_gate = false;
 	size_t j = i;
 	for(; j < count; ++j) {
 		std::vector<unsigned> qs;
-		std::vector<C> g;
+		std::vector<std::complex<double>> g;
 		if(!op_as_matrix(ops[j], qs, g)) break;
-		validate_op(h, ops[j]);
 		std::vector<unsigned> U = Q;
 		for(unsigned q : qs)
 			if(std::find(U.begin(), U.end(), q) == U.end()) U.push_back(q);
 		if(U.size() > 5) break;
 		Q = U;
+		has_gate = has_gate || ops[j].kind == TMFQS_OP_GATE;
+	}
+	return j;
+}
+
+// Starting at ops[i], the longest run of ops acting within 5 qubits (holding
+// a dense gate), multiplied in FP64 into one block matrix and applied in one
+// sweep: a tensor-core gate for complex64 (padded to 4 qubits), the CUDA-core
+// block kernel for the fast complex128 form.  Returns the number of ops
+// consumed (0: no block).
+size_t run_dense_block(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t i, size_t count) {
+	typedef std::complex<double> C;
+	if(!block_fusion(h)) return 0;
+	bool has_gate = false;
+	const size_t jend = dense_block_extent(h, ops, i, count, has_gate);
+	if(!has_gate || jend - i < 2) return 0;
+	std::vector<unsigned> Q;  // block qubits, block order (first = most significant)
+	std::vector<std::pair<std::vector<unsigned>, std::vector<C>>> parts;
+	size_t j = i;
+	for(; j < jend; ++j) {
+		std::vector<unsigned> qs;
+		std::vector<C> g;
+		op_as_matrix(ops[j], qs, g);
+		validate_op(h, ops[j]);
+		for(unsigned q : qs)
+			if(std::find(Q.begin(), Q.end(), q) == Q.end()) Q.push_back(q);
 		parts.push_back({qs, g});
 	}
-	if(parts.size() < 2) return 0;
-	// Pad to 4 qubits with the highest-order unused ones (identity on them).
-	for(unsigned q = 0; Q.size() < 4 && q < h->n; ++q)
-		if(std::find(Q.begin(), Q.end(), q) == Q.end()) Q.push_back(q);
+	const bool tensor = h->precision == TMFQS_FP32 && h->opt_tensor;
+	if(tensor) {
+		// Pad to 4 qubits with the highest-order unused ones (identity on them).
+		for(unsigned q = 0; Q.size() < 4 && q < h->n; ++q)
+			if(std::find(Q.begin(), Q.end(), q) == Q.end()) Q.push_back(q);
+		if(!tqb::tc_gate_supported(h->precision, h->n, (unsigned)Q.size())) return 0;
+	}
 	const unsigned s = (unsigned)Q.size();
-	if(!tqb::tc_gate_supported(h->precision, h->n, s)) return 0;
 	const size_t d = size_t(1) << s;
 	std::vector<C> M(d * d, C(0));
 	for(size_t r = 0; r < d; ++r) M[r * d + r] = C(1);
@@ -986,6 +1023,12 @@ size_t run_dense_block(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t i, size_t
 		mat[2 * e] = M[e].real();
 		mat[2 * e + 1] = M[e].imag();
 	}
+	h->cur_first = i;
+	h->cur_count = (unsigned)(j - i);
+	if(!tensor) {
+		run_gate(h, mat.data(), Q.data(), s);
+		return j - i;
+	}
 	std::vector<unsigned> tpos(s);
 	for(unsigned a = 0; a < s; ++a) tpos[a] = bit_of(h, Q[a]);
 	{
@@ -1006,9 +1049,18 @@ bool apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool 
 	if(count && !ops) fail(TMFQS_ERR_INVALID_ARGUMENT, "null op list");
 	DeviceScope d(h);
 	before_mutation(h);
+	struct RangeReset {
+		tmfqs_gpu_state *h;
+		~RangeReset() {
+			h->cur_first = 0;
+			h->cur_count = 0;
+		}
+	} range_reset{h};
 	if(!h->opt_fusion) {
 		for(size_t i = 0; i < count; ++i) {
 			validate_op(h, ops[i]);
+			h->cur_first = i;
+			h->cur_count = 1;
 			Planner p(h);
 			if(ops[i].kind == TMFQS_OP_GATE) run_gate(h, ops[i].matrix, ops[i].qubits, ops[i].k);
 			else p.run_single(ops[i]);
@@ -1020,6 +1072,7 @@ bool apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool 
 		return false;
 	}
 	Planner p(h);
+	p.base = ops;
 	size_t i = 0;
 	try {
 		while(i < count) {
@@ -1032,6 +1085,8 @@ bool apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool 
 					p.flush();
 					std::vector<std::pair<unsigned, unsigned>> pairs;
 					for(size_t j = i; j < i + run; ++j) pairs.push_back({bit_of(h, ops[j].q0), bit_of(h, ops[j].q1)});
+					h->cur_first = i;
+					h->cur_count = (unsigned)run;
 					{
 						PassTimer timer(h, TMFQS_KT_PERMUTE, sweep_bytes(h));
 						tqb::launch_bit_permutation(ctx(h), h->precision, h->amps, h->n, pairs);
@@ -1043,18 +1098,31 @@ bool apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool 
 			}
 			if(op.kind == TMFQS_OP_GATE) {
 				p.flush();
-				if(h->precision == TMFQS_FP32 && h->opt_tensor) {
-					// A dense gate and the ops after it that stay within 5 qubits:
-					// one block on the tensor cores.
+				h->cur_first = i;
+				h->cur_count = 1;
+				// A dense gate and the ops after it that stay within 5 qubits: one block sweep.
+				const size_t used = run_dense_block(h, ops, i, count);
+				if(used) {
+					i += used;
+					continue;
+				}
+				run_gate(h, op.matrix, op.qubits, op.k);
+				++i;
+				continue;
+			}
+			if(block_fusion(h)) {
+				// Gates that lead into a dense gate within the same 5 qubits join its block.
+				bool has_gate = false;
+				const size_t jend = dense_block_extent(h, ops, i, count, has_gate);
+				if(has_gate && jend - i >= 2) {
+					validate_op(h, op);
+					p.flush();
 					const size_t used = run_dense_block(h, ops, i, count);
 					if(used) {
 						i += used;
 						continue;
 					}
 				}
-				run_gate(h, op.matrix, op.qubits, op.k);
-				++i;
-				continue;
 			}
 			p.add(op);
 			++i;
@@ -1923,6 +1991,27 @@ int tmfqs_gpu_reset_stats(tmfqs_gpu_state *h) {
 		resolve_timers(h);
 		h->stats = tmfqs_stats{};
 		for(auto &t : h->times) t = tmfqs_kernel_time{};
+		h->pass_log.clear();
+		h->segment = 0;
+	});
+}
+
+int tmfqs_gpu_pass_mark(tmfqs_gpu_state *h, uint64_t *segment_out) {
+	return guarded([&] {
+		require_handle(h);
+		++h->segment;
+		if(segment_out) *segment_out = h->segment;
+	});
+}
+
+int tmfqs_gpu_pass_log(tmfqs_gpu_state *h, tmfqs_pass_record *out, size_t capacity, size_t *count) {
+	return guarded([&] {
+		require_handle(h);
+		if(!count) fail(TMFQS_ERR_INVALID_ARGUMENT, "null count");
+		DeviceScope d(h);
+		resolve_timers(h);
+		*count = h->pass_log.size();
+		if(out) std::copy(h->pass_log.begin(), h->pass_log.begin() + std::min(capacity, h->pass_log.size()), out);
 	});
 }
 

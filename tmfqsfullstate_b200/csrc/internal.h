@@ -294,9 +294,16 @@ struct tmfqs_gpu_state {
 		int kind;
 		cudaEvent_t start, stop;
 		double bytes;
+		uint64_t segment, first;
+		unsigned count;
 	};
 	std::vector<TimedLaunch> timed;
 	tmfqs_kernel_time times[TMFQS_KT_COUNT] = {};
+	// Pass log (tmfqs_gpu_pass_log): the op range of the launch being issued
+	// (within the current apply_ops call; count 0 outside gate batches).
+	uint64_t segment = 0, cur_first = 0;
+	unsigned cur_count = 0;
+	std::vector<tmfqs_pass_record> pass_log;
 	bool opt_fusion = true;
 	int opt_fused_qubits = 0;  // 0 = default by precision
 	bool opt_grover_fusion = true;

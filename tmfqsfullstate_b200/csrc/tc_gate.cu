@@ -17,7 +17,9 @@
 // after the MMAs reads its row of D back from tensor memory (warp w reads
 // lanes 32w..32w+31) and stores the outputs to the same addresses.  One
 // elected thread issues the MMAs; their completion arrives on an mbarrier
-// whose wait is bounded (a timeout sets an error flag instead of hanging).
+// whose wait is bounded: a timeout sets an error flag instead of hanging,
+// stops the tile loop, and waits (bounded again) for the outstanding MMAs
+// before the tensor memory is released.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gate(float2 *a, TcGateGeom g,
 	const uint32_t tbase = tmem_base;
 	const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((N >> 3) << 17) | ((kTcRows >> 4) << 24);
 	bool ok = true;
-	uint32_t phase = 0;
+	uint32_t phase = 0, stuck_phase = 0;
 	// This thread's group in a tile: its non-target bits are the index, targets zero.
 	auto group_base = [&](uint64_t tile) {
 		uint64_t gb = tile * kTcRows + tid;
@@ -171,6 +173,7 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gate(float2 *a, TcGateGeom g,
 		if(__syncthreads_or(!done)) {
 			if(tid == 0) atomicExch(err, 1);
 			ok = false;
+			stuck_phase = phase;
 		}
 		asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 		if(ok) {
@@ -189,6 +192,17 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gate(float2 *a, TcGateGeom g,
 		__syncthreads();
 #pragma unroll
 		for(int c = 0; c < D; ++c) x[c] = xn[c];
+	}
+	if(!ok) {
+		// The MMAs of the tile that timed out may still be running: wait for
+		// their completion once more (bounded too) before the accumulator's
+		// tensor memory is released, so no MMA writes a freed allocation.
+		uint32_t done = 0;
+		for(int it = 0; it < (1 << 22) && !done; ++it)
+			asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}"
+			             : "=r"(done) : "r"(smem_u32(&mbar)), "r"(stuck_phase) : "memory");
+		if(tid == 0 && !done) atomicExch(err, 2);
+		asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 	}
 	__syncthreads();
 	if(warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TCOLS));
@@ -295,7 +309,8 @@ void launch_tc_gate(const LaunchCtx &c, void *a, unsigned n, unsigned k, const d
 	int herr = 0;
 	check_cuda(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, c.stream), "tensor gate flag read");
 	check_cuda(cudaStreamSynchronize(c.stream), "tensor gate sync");
-	if(herr) fail(TMFQS_ERR_RUNTIME, "tensor-core gate: MMA completion wait timed out");
+	if(herr == 1) fail(TMFQS_ERR_RUNTIME, "tensor-core gate: MMA completion wait timed out (drained before release)");
+	if(herr) fail(TMFQS_ERR_RUNTIME, "tensor-core gate: MMA completion wait timed out, and so did the drain");
 }
 
 }  // namespace tqb

@@ -24,6 +24,9 @@ struct StateComparison {
 };
 
 StateComparison compareStates(const state::QuantumState &reference, const state::QuantumState &candidate);
+// The same metrics by one bulk read of both states on the host, whatever
+// holds them (compareStates uses it when the states are not both on a device).
+StateComparison compareStatesOnHost(const state::QuantumState &reference, const state::QuantumState &candidate);
 std::string toCsvRow(const std::string &circuit, const std::string &scenario, unsigned int qubits, const StateComparison &comparison);
 std::string toJson(const StateComparison &comparison);
 

@@ -19,6 +19,17 @@
 namespace tmfqs {
 
 class IRandomSource;
+class QuantumRegister;
+namespace sim {
+class Simulator;
+}
+namespace state {
+class QuantumState;
+}
+namespace experiment {
+struct StateComparison;
+StateComparison compareStates(const state::QuantumState &reference, const state::QuantumState &candidate);
+}
 
 class QuantumRegister {
 	public:
@@ -73,6 +84,19 @@ class QuantumRegister {
 		void applyGroverIterations(const std::vector<StateIndex> &sortedMarked, uint64_t iterations, bool materialized);
 
 	private:
+		friend class sim::Simulator;
+		friend experiment::StateComparison experiment::compareStates(const state::QuantumState &, const state::QuantumState &);
+		// Device pass traces (Simulator with traceOperations) and in-place
+		// comparison of two device states without a lazy overlay.
+		bool beginPassTrace() { return backend_ && backend_->beginPassTrace(); }
+		uint64_t markPassSegment() { return backend_->markPassSegment(); }
+		bool endPassTrace(std::vector<BackendPassTrace> &out) { return backend_->endPassTrace(out); }
+		bool compareOnDevice(const QuantumRegister &candidate, BackendComparison &out) const {
+			if(!backend_ || !candidate.backend_ || affineOverlayActive_ || candidate.affineOverlayActive_) return false;
+			if(numQubits_ != candidate.numQubits_) return false;
+			return backend_->compareWith(*candidate.backend_, out);
+		}
+
 		unsigned int numQubits_ = 0;
 		StateIndex numStates_ = 0;
 		RegisterConfig config_{};

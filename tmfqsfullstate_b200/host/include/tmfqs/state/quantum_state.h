@@ -16,6 +16,13 @@ class QuantumRegister;
 namespace sim {
 class Simulator;
 }
+namespace state {
+class QuantumState;
+}
+namespace experiment {
+struct StateComparison;
+StateComparison compareStates(const state::QuantumState &reference, const state::QuantumState &candidate);
+}
 
 namespace state {
 
@@ -59,6 +66,9 @@ class QuantumState {
 		QuantumRegister materialize(const RegisterConfig &config) const;
 		static QuantumState fromRegister(QuantumRegister reg);
 		friend class tmfqs::sim::Simulator;
+		friend experiment::StateComparison experiment::compareStates(const QuantumState &, const QuantumState &);
+		// The device register holding this state, if it is a simulation result.
+		const QuantumRegister *registerOrNull() const;
 };
 
 }  // namespace state

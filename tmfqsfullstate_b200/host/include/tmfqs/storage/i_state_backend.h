@@ -9,6 +9,7 @@
 #include <functional>
 #include <iosfwd>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "tmfqs/core/types.h"
@@ -43,6 +44,24 @@ struct RegisterSideState {
 	Amplitude sum{0.0, 0.0};
 	bool overlayActive = false;
 	AffineOverlay overlay;
+};
+
+// One timed device pass of a traced run (see IStateBackend::endPassTrace).
+struct BackendPassTrace {
+	std::string kind;       // "fused", "permute", "gate", "reduce", "grover"
+	uint64_t segment = 0;   // the markPassSegment() number it ran under
+	uint64_t firstOp = 0;   // first operation within its applyOperationRun call
+	unsigned opCount = 0;   // operations it applied (0: not an operation run)
+	double seconds = 0.0;   // device time (CUDA events)
+};
+
+// experiment::StateComparison's fields, filled by a backend that compares two
+// of its states in place.
+struct BackendComparison {
+	bool bitwiseEqual = false;
+	double maxAbsAmplitudeError = 0.0, maxAbsComponentError = 0.0, rmseAmplitude = 0.0, relL2 = 0.0,
+	       maxAbsProbabilityError = 0.0, totalProbabilityDiff = 0.0;
+	StateIndex worstState = 0u;
 };
 
 class IStateBackend {
@@ -89,6 +108,13 @@ class IStateBackend {
 		// `iterations` Grover iterations over sorted unique marked states with
 		// QuantumRegister's exact semantics, updating `side`.
 		virtual bool runGroverIterations(RegisterSideState &, const std::vector<StateIndex> &, uint64_t, bool) { return false; }
+		// Per-pass device timing for traced runs: begin, mark each backend call
+		// (segment), then collect the passes; the batching hooks stay in use.
+		virtual bool beginPassTrace() { return false; }
+		virtual uint64_t markPassSegment() { return 0; }
+		virtual bool endPassTrace(std::vector<BackendPassTrace> &) { return false; }
+		// experiment::compareStates on two states of this backend, in place.
+		virtual bool compareWith(const IStateBackend &, BackendComparison &) const { return false; }
 };
 
 }  // namespace tmfqs

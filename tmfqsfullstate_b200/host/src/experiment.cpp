@@ -8,6 +8,7 @@
 
 #include "tmfqs/experiment/comparison.h"
 #include "tmfqs/experiment/report.h"
+#include "tmfqs/register/quantum_register.h"
 #include "tmfqs/storage/factory/storage_strategy_registry.h"
 
 namespace tmfqs {
@@ -74,9 +75,31 @@ std::string toCsv(const RunReport &r) {
 void writeJsonReport(const RunReport &r, const std::string &path) { writeFile(path, toJson(r)); }
 void writeCsvReport(const RunReport &r, const std::string &path) { writeFile(path, toCsv(r)); }
 
-// Metrics of comparison.cpp:12-62; both states are read once in bulk (the
-// reference reads them one amplitude at a time).
+// Metrics of comparison.cpp:12-62.  When both states are device registers
+// (simulation results without a lazy overlay), the comparison runs on the
+// device (tmfqs_gpu_compare: every field equal to the host loop's, the sums
+// replayed in the reference's order); otherwise both states are read once in
+// bulk (the reference reads them one amplitude at a time).
 StateComparison compareStates(const state::QuantumState &reference, const state::QuantumState &candidate) {
+	if(reference.stateCount() != candidate.stateCount()) throw std::invalid_argument("Compared states must have the same state count");
+	const QuantumRegister *rr = reference.registerOrNull(), *cr = candidate.registerOrNull();
+	BackendComparison dev;
+	if(rr && cr && rr->compareOnDevice(*cr, dev)) {
+		StateComparison m;
+		m.bitwiseEqual = dev.bitwiseEqual;
+		m.maxAbsAmplitudeError = dev.maxAbsAmplitudeError;
+		m.maxAbsComponentError = dev.maxAbsComponentError;
+		m.rmseAmplitude = dev.rmseAmplitude;
+		m.relL2 = dev.relL2;
+		m.maxAbsProbabilityError = dev.maxAbsProbabilityError;
+		m.totalProbabilityDiff = dev.totalProbabilityDiff;
+		m.worstState = dev.worstState;
+		return m;
+	}
+	return compareStatesOnHost(reference, candidate);
+}
+
+StateComparison compareStatesOnHost(const state::QuantumState &reference, const state::QuantumState &candidate) {
 	if(reference.stateCount() != candidate.stateCount()) throw std::invalid_argument("Compared states must have the same state count");
 	const AmplitudesVector ref = reference.amplitudes();
 	const AmplitudesVector got = candidate.amplitudes();

@@ -251,6 +251,10 @@ QuantumRegister QuantumState::materialize(const RegisterConfig &cfg) const {
 	return QuantumRegister(impl_->qubits, cfg);
 }
 
+const QuantumRegister *QuantumState::registerOrNull() const {
+	return impl_->kind == Kind::Register ? impl_->reg.get() : nullptr;
+}
+
 QuantumState QuantumState::fromRegister(QuantumRegister reg) {
 	auto impl = std::make_unique<Impl>();
 	impl->qubits = reg.qubitCount();

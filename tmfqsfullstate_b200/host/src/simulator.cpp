@@ -3,13 +3,18 @@
 // (fused multi-gate passes on the device) and repeated Grover iterations --
 // sorted unique phase flips followed by an inversion about the mean -- go to
 // QuantumRegister::applyGroverIterations.  Both have exactly the results of
-// executing the operations one by one.  With traceOperations on, operations
-// run one at a time and each is synchronised, so per-operation times measure
+// executing the operations one by one.  With traceOperations on, a backend
+// that times its device passes (CUDA events) keeps the batching, and the
+// report holds one trace per device pass: its first circuit operation, the
+// operations it applied, and its device time.  Other backends run the
+// operations one at a time, each synchronised, so per-operation times measure
 // device work rather than enqueue time.
 #include "tmfqs/sim/simulator.h"
 
+#include <algorithm>
 #include <chrono>
 #include <stdexcept>
+#include <string>
 #include <type_traits>
 #include <utility>
 
@@ -96,7 +101,14 @@ bool toBackendOp(const circuit::Operation &operation, BackendOp &out) {
 	return ok;
 }
 
-void executeBatched(QuantumRegister &reg, const std::vector<circuit::Operation> &ops) {
+// A backend call of a traced run: the circuit operations [first, first + count).
+struct Segment {
+	size_t first, count;
+};
+
+// `mark` (traced runs) is called before each backend call with its operation range.
+template <typename Mark>
+void executeBatched(QuantumRegister &reg, const std::vector<circuit::Operation> &ops, Mark &&mark) {
 	std::vector<StateIndex> marked;
 	bool materialized = false;
 	size_t i = 0;
@@ -105,12 +117,14 @@ void executeBatched(QuantumRegister &reg, const std::vector<circuit::Operation> 
 		if(len) {
 			uint64_t reps = 1;
 			while(samePattern(ops, i + reps * len, len, marked, materialized)) ++reps;
+			mark(i, reps * len);
 			reg.applyGroverIterations(marked, reps, materialized);
 			i += reps * len;
 			continue;
 		}
 		std::vector<BackendOp> run;
 		BackendOp b;
+		const size_t first = i;
 		while(i < ops.size() && toBackendOp(ops[i], b)) {
 			std::vector<StateIndex> probe;
 			bool m = false;
@@ -119,12 +133,31 @@ void executeBatched(QuantumRegister &reg, const std::vector<circuit::Operation> 
 			++i;
 		}
 		if(!run.empty()) {
+			mark(first, run.size());
 			reg.applyOperationRun(run);
 			continue;
 		}
+		mark(i, 1);
 		executeOperation(reg, ops[i]);
 		++i;
 	}
+}
+
+// "fused: h, controlled_phase x15, h" -- the operation names of [first, first + count), repeats folded.
+std::string passName(const std::string &kind, const std::vector<circuit::Operation> &ops, size_t first, size_t count) {
+	std::string out = kind + ":";
+	size_t k = first;
+	const size_t end = std::min(ops.size(), first + count);
+	bool firstName = true;
+	while(k < end) {
+		const std::string name = circuit::operationName(ops[k]);
+		size_t r = 1;
+		while(k + r < end && circuit::operationName(ops[k + r]) == name) ++r;
+		out += (firstName ? " " : ", ") + name + (r > 1 ? " x" + std::to_string(r) : "");
+		firstName = false;
+		k += r;
+	}
+	return out;
 }
 
 }  // namespace
@@ -148,7 +181,23 @@ RunResult Simulator::run(const circuit::Circuit &circuit, const state::QuantumSt
 	bool open = true;
 	try {
 		const std::vector<circuit::Operation> &ops = circuit.operations();
-		if(config_.observability.traceOperations) {
+		if(config_.observability.traceOperations && reg.beginPassTrace()) {
+			std::vector<Segment> segments;  // segment s (numbered from 1) = segments[s - 1]
+			executeBatched(reg, ops, [&](size_t first, size_t count) {
+				reg.markPassSegment();
+				segments.push_back({first, count});
+			});
+			reg.endOperationBatch();
+			std::vector<BackendPassTrace> passes;
+			reg.endPassTrace(passes);
+			for(const BackendPassTrace &p : passes) {
+				if(p.segment == 0 || p.segment > segments.size()) continue;
+				const Segment &sg = segments[p.segment - 1];
+				const size_t first = p.opCount ? sg.first + p.firstOp : sg.first;
+				const size_t count = p.opCount ? p.opCount : sg.count;
+				report.operations.push_back({first, passName(p.kind, ops, first, count), p.seconds});
+			}
+		} else if(config_.observability.traceOperations) {
 			for(size_t i = 0; i < ops.size(); ++i) {
 				const auto t0 = Clock::now();
 				executeOperation(reg, ops[i]);
@@ -156,7 +205,7 @@ RunResult Simulator::run(const circuit::Circuit &circuit, const state::QuantumSt
 				report.operations.push_back({i, circuit::operationName(ops[i]), std::chrono::duration<double>(Clock::now() - t0).count()});
 			}
 		} else {
-			executeBatched(reg, ops);
+			executeBatched(reg, ops, [](size_t, size_t) {});
 		}
 		reg.endOperationBatch();
 		open = false;

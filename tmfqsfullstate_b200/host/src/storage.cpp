@@ -177,6 +177,52 @@ class GpuStateBackend final : public IStateBackend {
 			return true;
 		}
 
+		bool beginPassTrace() override {
+			check(tmfqs_gpu_sync(h_));
+			check(tmfqs_gpu_reset_stats(h_));
+			check(tmfqs_gpu_set_option(h_, TMFQS_OPT_KERNEL_TIMING, 1));
+			return true;
+		}
+		uint64_t markPassSegment() override {
+			uint64_t seg = 0;
+			check(tmfqs_gpu_pass_mark(h_, &seg));
+			return seg;
+		}
+		bool endPassTrace(std::vector<BackendPassTrace> &out) override {
+			static const char *kKinds[] = {"fused", "permute", "gate", "reduce", "grover", "adjoint"};
+			size_t n = 0;
+			check(tmfqs_gpu_pass_log(h_, nullptr, 0, &n));
+			std::vector<tmfqs_pass_record> recs(n);
+			check(tmfqs_gpu_pass_log(h_, recs.data(), n, &n));
+			check(tmfqs_gpu_set_option(h_, TMFQS_OPT_KERNEL_TIMING, 0));
+			out.clear();
+			for(const tmfqs_pass_record &r : recs) {
+				BackendPassTrace t;
+				t.kind = (r.kind >= 0 && r.kind < 6) ? kKinds[r.kind] : "pass";
+				t.segment = r.segment;
+				t.firstOp = r.first_op;
+				t.opCount = r.op_count;
+				t.seconds = r.ms * 1e-3;
+				out.push_back(t);
+			}
+			return true;
+		}
+		bool compareWith(const IStateBackend &candidate, BackendComparison &out) const override {
+			const auto *o = dynamic_cast<const GpuStateBackend *>(&candidate);
+			if(!o) return false;
+			tmfqs_state_comparison c{};
+			check(tmfqs_gpu_compare(h_, o->h_, &c));
+			out.bitwiseEqual = c.bitwise_equal != 0;
+			out.maxAbsAmplitudeError = c.max_abs_amplitude_error;
+			out.maxAbsComponentError = c.max_abs_component_error;
+			out.rmseAmplitude = c.rmse_amplitude;
+			out.relL2 = c.rel_l2;
+			out.maxAbsProbabilityError = c.max_abs_probability_error;
+			out.totalProbabilityDiff = c.total_probability_diff;
+			out.worstState = c.worst_state;
+			return true;
+		}
+
 	private:
 		GpuStateBackend(const GpuConfig &cfg, tmfqs_gpu_state *h, unsigned n) : h_(h), n_(n), cfg_(cfg) {}
 

@@ -10,6 +10,9 @@
 #include <sstream>
 #include <stdexcept>
 #include <vector>
+#include <string>
+#include <variant>
+#include <type_traits>
 
 #include "tmfqsfs.h"
 #include "tmfqs_b200.h"
@@ -203,6 +206,43 @@ void registryAndCopies() {
 // The batched Simulator path and the per-operation path give bit-identical
 // amplitudes, totals and measurements (gate runs, swaps, matrix gates,
 // flips, both diffusion forms).
+// The circuit one operation at a time through QuantumRegister's public API
+// (no batching hooks): the per-operation path the batched one must equal.
+QuantumRegister runPerOperation(const circuit::Circuit &c, const state::QuantumState &in) {
+	QuantumRegister reg(in.qubitCount(), in.amplitudes());
+	for(const circuit::Operation &operation : c.operations())
+		std::visit(
+			[&](const auto &op) {
+				using Op = std::decay_t<decltype(op)>;
+				if constexpr(std::is_same<Op, circuit::Hadamard>::value) reg.applyHadamard(op.target);
+				else if constexpr(std::is_same<Op, circuit::PauliX>::value) reg.applyPauliX(op.target);
+				else if constexpr(std::is_same<Op, circuit::ControlledNot>::value) reg.applyControlledNot(op.control, op.target);
+				else if constexpr(std::is_same<Op, circuit::ControlledPhaseShift>::value)
+					reg.applyControlledPhaseShift(op.control, op.target, op.theta);
+				else if constexpr(std::is_same<Op, circuit::Swap>::value) reg.applySwap(op.first, op.second);
+				else if constexpr(std::is_same<Op, circuit::MatrixGate>::value) reg.applyGate(op.gate, op.targets);
+				else if constexpr(std::is_same<Op, circuit::PhaseFlipBasisState>::value) reg.applyPhaseFlipBasisState(op.state);
+				else if constexpr(std::is_same<Op, circuit::InversionAboutMean>::value) {
+					if(op.materialized) reg.applyInversionAboutMeanMaterialized();
+					else reg.applyInversionAboutMean();
+				}
+			},
+			operation);
+	return reg;
+}
+
+// A traced run keeps the fused passes: one trace per device pass, at its first
+// circuit operation, in circuit order, with a positive device time.
+void checkPassTraces(const experiment::RunReport &rep, size_t ops) {
+	REQUIRE(!rep.operations.empty() && rep.operations.size() <= ops);
+	REQUIRE(rep.operations.front().index == 0);
+	for(size_t k = 0; k < rep.operations.size(); ++k) {
+		const experiment::OperationTrace &t = rep.operations[k];
+		REQUIRE(t.index < ops && t.seconds > 0.0 && t.name.find(':') != std::string::npos);
+		if(k) REQUIRE(t.index >= rep.operations[k - 1].index);
+	}
+}
+
 void batchedEqualsPerOperation() {
 	for(unsigned n : {3u, 6u, 11u, 14u}) {
 		circuit::Circuit c(n);
@@ -217,13 +257,17 @@ void batchedEqualsPerOperation() {
 		const state::QuantumState in = state::QuantumState::randomPhase(n, 7u + n);
 		const sim::RunResult a = sim::Simulator().run(c, in);
 		const sim::RunResult b = sim::Simulator(traced).run(c, in);
-		const AmplitudesVector va = a.state.amplitudes(), vb = b.state.amplitudes();
-		REQUIRE(va.size() == vb.size());
+		const QuantumRegister per = runPerOperation(c, in);
+		const AmplitudesVector va = a.state.amplitudes(), vb = b.state.amplitudes(), vp = per.amplitudes();
+		REQUIRE(va.size() == vb.size() && va.size() == vp.size());
 		REQUIRE(std::memcmp(va.data(), vb.data(), va.size() * sizeof(double)) == 0 || va == vb);
+		REQUIRE(std::memcmp(va.data(), vp.data(), va.size() * sizeof(double)) == 0 || va == vp);
 		REQUIRE(a.state.totalProbability() == b.state.totalProbability());
-		Mt19937RandomSource r1(99u), r2(99u);
-		REQUIRE(a.state.measure(r1) == b.state.measure(r2));
-		REQUIRE(b.report.operations.size() == c.operationCount());
+		REQUIRE(a.state.totalProbability() == per.totalProbability());
+		Mt19937RandomSource r1(99u), r2(99u), r3(99u);
+		const StateIndex m1 = a.state.measure(r1);
+		REQUIRE(m1 == b.state.measure(r2) && m1 == per.measure(r3));
+		checkPassTraces(b.report, c.operationCount());
 	}
 	for(bool mat : {true, false}) {
 		circuit::GroverCircuitOptions o;
@@ -234,9 +278,51 @@ void batchedEqualsPerOperation() {
 		traced.observability.traceOperations = true;
 		const sim::RunResult a = sim::Simulator().run(c, state::QuantumState::basis(12));
 		const sim::RunResult b = sim::Simulator(traced).run(c, state::QuantumState::basis(12));
+		const QuantumRegister per = runPerOperation(c, state::QuantumState::basis(12));
 		REQUIRE(a.state.amplitudes() == b.state.amplitudes());
+		REQUIRE(a.state.amplitudes() == per.amplitudes());
 		REQUIRE(a.state.totalProbability() == b.state.totalProbability());
+		checkPassTraces(b.report, c.operationCount());
 	}
+	// QFT-16: the passes of the fused plan (three fused passes and the bit
+	// reversal), their names covering the circuit's operations.
+	circuit::Circuit q(16);
+	circuit::appendQft(q);
+	sim::ExecutionConfig traced;
+	traced.observability.traceOperations = true;
+	const sim::RunResult t = sim::Simulator(traced).run(q, state::QuantumState::randomPhase(16, 5u));
+	checkPassTraces(t.report, q.operationCount());
+	REQUIRE(t.report.operations.size() <= 8);
+	REQUIRE(t.report.operations.back().name == "permute: swap x8");
+}
+
+// experiment::compareStates of two device results runs on the device and
+// equals the host loop field for field; with a lazy overlay active it falls
+// back to the host.
+void deviceCompareStates() {
+	circuit::Circuit c(14);
+	circuit::appendQft(c);
+	const state::QuantumState in = state::QuantumState::randomPhase(14, 3u);
+	const sim::RunResult a = sim::Simulator().run(c, in);
+	sim::ExecutionConfig fast;
+	fast.backend.gpu.exact = false;
+	const sim::RunResult b = sim::Simulator(fast).run(c, in);
+	const experiment::StateComparison dev = experiment::compareStates(a.state, b.state);
+	const experiment::StateComparison host = experiment::compareStatesOnHost(a.state, b.state);
+	REQUIRE(dev.bitwiseEqual == host.bitwiseEqual && dev.worstState == host.worstState);
+	REQUIRE(dev.maxAbsAmplitudeError == host.maxAbsAmplitudeError && dev.maxAbsComponentError == host.maxAbsComponentError);
+	REQUIRE(dev.maxAbsProbabilityError == host.maxAbsProbabilityError);
+	REQUIRE(dev.relL2 == host.relL2 && dev.rmseAmplitude == host.rmseAmplitude);
+	REQUIRE(dev.totalProbabilityDiff == host.totalProbabilityDiff);
+	REQUIRE(!dev.bitwiseEqual && dev.relL2 > 0.0 && dev.relL2 < 1e-12);
+	const experiment::StateComparison same = experiment::compareStates(a.state, a.state);
+	REQUIRE(same.bitwiseEqual && same.relL2 == 0.0);
+	circuit::GroverCircuitOptions o;
+	o.markedStates = {77};
+	const circuit::Circuit g = circuit::makeGrover(10, o);  // lazy diffusion: overlay active at the end
+	const sim::RunResult ga = sim::Simulator().run(g, state::QuantumState::basis(10));
+	const experiment::StateComparison gd = experiment::compareStates(ga.state, ga.state);
+	REQUIRE(gd.bitwiseEqual && gd.relL2 == 0.0);
 }
 
 void operationsAndSwaps() {
@@ -294,6 +380,7 @@ int main() {
 		batchedEqualsPerOperation();
 		operationsAndSwaps();
 		failureMapping();
+		deviceCompareStates();
 	} catch(const std::exception &e) {
 		std::cout << "FAILED after " << g_checks << " checks: " << e.what() << "\n";
 		return 1;
