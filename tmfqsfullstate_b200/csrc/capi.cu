@@ -443,6 +443,13 @@ struct Planner {
 	// local indices once the local set is known.
 	void flush() {
 		if(pending.empty()) return;
+		// The pass is consumed whether or not its launch succeeds: a failed
+		// launch must not leave its (already converted) ops pending for the
+		// error path's flush of the ops before a failing one.
+		struct Consume {
+			Planner *p;
+			~Consume() { p->reset(); }
+		} consume{this};
 		if(base) {
 			h->cur_first = (uint64_t)(pending.front() - base);
 			h->cur_count = (unsigned)pending.size();
@@ -480,7 +487,6 @@ struct Planner {
 			if(!done) tqb::launch_fused_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes);
 			++h->stats.fused_passes;
 		}
-		reset();
 	}
 
 	void run_single(const tmfqs_op &op) {
