@@ -574,6 +574,14 @@ def run_unmodified_simulator(n, fused_ms):
     return r
 
 
+def _section(name, fn, *a, **k):
+    """Runs one report section, logging its wall time to stderr."""
+    t0 = time.perf_counter()
+    out = fn(*a, **k)
+    print(f"[bench] {name}: {time.perf_counter() - t0:.1f} s", file=sys.stderr, flush=True)
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -705,19 +713,20 @@ def run_ours(args):
 
     adjoint = None
     if rank == 0 and not args.no_adjoint:
-        adjoint = run_adjoint(tq, torch, local)
+        adjoint = _section("adjoint", run_adjoint, tq, torch, local)
     configs = None
     if rank == 0 and not args.no_configs:
-        configs = {"qft32": run_qft32(tq, torch, local, peak), "grover30": run_grover30(tq, torch, local, peak),
+        configs = {"qft32": _section("qft32", run_qft32, tq, torch, local, peak),
+                   "grover30": _section("grover30", run_grover30, tq, torch, local, peak),
                    "block_gate": run_block_gate(tq, torch, local, peak)}
 
     dropin = None
     if rank == 0 and not args.no_dropin:
-        dropin = run_unmodified_simulator(n, ms_per_step)
+        dropin = _section("unmodified_simulator", run_unmodified_simulator, n, ms_per_step)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(n)
+        cpu = _section("cpu_baseline", cpu_baseline, n)
 
     g.close()
     if rank == 0:
