@@ -709,6 +709,11 @@ def run_ours(args):
             forms[name] = run_form(tq, torch, n, inp, ops, prec, exact, max(1, args.form_steps), peak, plain, rnd,
                                    local, qp)
             forms[name]["speedup_vs_plain"] = (ms_per_step / forms[name]["ms_per_qft"])
+        # complex64 against both complex128 forms: the exact one (bit-identical to the
+        # reference) and the fast one (relL2 <= 1e-12), same GPU, same run.
+        forms["speedup_complex64_vs_complex128_exact"] = forms["complex64_radix"]["speedup_vs_plain"]
+        forms["speedup_complex64_vs_complex128_fast"] = (forms["complex128_fast"]["ms_per_qft"] /
+                                                         forms["complex64_radix"]["ms_per_qft"])
         del plain
 
     adjoint = None
