@@ -178,6 +178,16 @@ TMFQS_API int tmfqs_gpu_init_uniform(tmfqs_gpu_state *h, unsigned num_qubits, co
 /* loadAmplitudes, i_state_backend.h:56: 2^(n+1) doubles from host memory. */
 TMFQS_API int tmfqs_gpu_load(tmfqs_gpu_state *h, unsigned num_qubits, const double *host_amps);
 /* Loads `count` amplitudes starting at `first_state` into an initialised state. */
+/* loadAmplitudes followed by a gate batch (tmfqs_gpu_apply_ops), for a caller
+ * that holds the whole input on the host -- IStateBackend::loadAmplitudes
+ * (i_state_backend.h:56) and the run of Simulator::run that follows it
+ * (simulator.cpp:72-82).  Same results and errors as tmfqs_gpu_load then
+ * tmfqs_gpu_apply_ops; for an exact complex128 batch that starts with a fused
+ * pass the host-to-device copy goes in slabs on a second stream and the first
+ * pass runs each slab's tiles as soon as it lands.  `host` must stay valid until
+ * the call returns (pinned memory lets the slabs overlap the pass). */
+TMFQS_API int tmfqs_gpu_load_apply_ops(tmfqs_gpu_state *h, unsigned num_qubits, const double *host, const tmfqs_op *ops,
+                                       size_t count);
 TMFQS_API int tmfqs_gpu_load_chunk(tmfqs_gpu_state *h, uint64_t first_state, const double *host_amps, uint64_t count);
 /* exportAmplitudes, i_state_backend.h:61. */
 TMFQS_API int tmfqs_gpu_export(tmfqs_gpu_state *h, double *host_out);

@@ -10,9 +10,10 @@ does), its CLIs and a QFT driver against it.  Here they run on the GPU:
   every register those programs create -- explicit Dense ones included -- on
   the device backend; each must pass and must have created device backends;
 * the reference's qftG / grover / groverLazy CLIs with `--strategy gpu`;
-* the QFT through the reference's own Simulator and QuantumRegister (one
-  backend call per operation) on both strategies: identical total
-  probability and seeded measurement on the random-phase input.
+* the QFT (random-phase input) and Grover-20 (configuration 1, both
+  diffusion forms) through the reference's own Simulator and QuantumRegister
+  (one backend call per operation) on both strategies: identical total
+  probability and seeded measurement.
 """
 import json
 import os
@@ -72,3 +73,15 @@ def test_qft_through_the_reference_simulator_matches_dense(n):
     assert out["gpu"]["operations"] == out["dense"]["operations"] == n + n * (n - 1) // 2 + n // 2
     assert out["gpu"]["total_probability"] == out["dense"]["total_probability"]
     assert out["gpu"]["measured"] == out["dense"]["measured"]
+
+
+@pytest.mark.parametrize("materialized", [1, 0])
+def test_grover20_through_the_reference_simulator_matches_dense(materialized):
+    out = {}
+    for strategy in ("dense", "gpu"):
+        p = _run(["qft_through_simulator", "grover", "20", strategy, "524287", str(materialized)])
+        assert p.returncode == 0, p.stdout + p.stderr
+        out[strategy] = json.loads(p.stdout.strip().splitlines()[-1])
+    assert out["gpu"]["operations"] == out["dense"]["operations"]
+    assert out["gpu"]["total_probability"] == out["dense"]["total_probability"]
+    assert out["gpu"]["measured"] == out["dense"]["measured"] == 524287

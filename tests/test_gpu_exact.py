@@ -360,3 +360,32 @@ def test_init_io_cache_and_errors(gpu):
         b[6:16] = a[100:110]
         assert_same(g.export(), b, "load chunk")
         c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [10, 16, 21])
+def test_load_apply_ops_equals_load_then_apply(n):
+    """tmfqs_gpu_load_apply_ops (copy in slabs overlapped with the first pass)
+    gives the same bytes as load + apply_ops, for the QFT and a circuit whose
+    first pass is not a fused pass; and the same error after the same prefix."""
+    amps = O.random_phase(n, 40 + n)
+    for ops in (tq.qft_ops(n), [tq.swap(0, n - 1), tq.h(1)] + tq.qft_ops(n)):
+        with tq.GpuState(tq.FP64) as a, tq.GpuState(tq.FP64) as b:
+            a.load_apply_ops(n, amps, ops)
+            b.load(n, amps)
+            b.apply_ops(ops)
+            assert np.array_equal(a.export(), b.export())
+            assert a.total_probability() == b.total_probability()
+    bad = tq.qft_ops(n)[:5] + [tq.h(n)] + tq.qft_ops(n)
+    with tq.GpuState(tq.FP64) as a, tq.GpuState(tq.FP64) as b:
+        with pytest.raises(tq.OutOfRange):
+            a.load_apply_ops(n, amps, bad)
+        b.load(n, amps)
+        with pytest.raises(tq.OutOfRange):
+            b.apply_ops(bad)
+        assert np.array_equal(a.export(), b.export())
+    with tq.GpuState(tq.FP32) as a, tq.GpuState(tq.FP32) as b:
+        a.load_apply_ops(n, amps, tq.qft_ops(n))
+        b.load(n, amps)
+        b.apply_ops(tq.qft_ops(n))
+        assert np.array_equal(a.export(), b.export())

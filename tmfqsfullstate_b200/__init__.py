@@ -189,6 +189,7 @@ SIGNATURES = {
     "tmfqs_sample_static": [ctypes.c_void_p, ctypes.c_int, _UI, _D, ctypes.c_void_p, _U64P],
     "tmfqs_debug_fail_allocations": [_UI, _UI],
     "tmfqs_gpu_pass_mark": [_H, _U64P],
+    "tmfqs_gpu_load_apply_ops": [_H, _UI, _DP, ctypes.c_void_p, ctypes.c_size_t],
     "tmfqs_gpu_pass_log": [_H, ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)],
     "tmfqs_mt19937_unit": [ctypes.c_uint32, _U64, _DP],
     "tmfqs_uniform_states": [_U64, _U64, _U64, _U64, _U64P],
@@ -572,6 +573,12 @@ class GpuState:
         arr = (KernelTime * len(KT_NAMES))()
         _check(lib().tmfqs_gpu_kernel_times(self._h, arr))
         return {n: {"launches": arr[i].launches, "ms": arr[i].ms, "bytes": arr[i].bytes} for i, n in enumerate(KT_NAMES)}
+
+    def load_apply_ops(self, n, amps: np.ndarray, ops):
+        """load(n, amps) then apply_ops(ops), with the copy overlapped with the first pass."""
+        assert amps.dtype == np.float64 and amps.size == 2 << n and amps.flags.c_contiguous
+        arr = op_array(ops)
+        _check(lib().tmfqs_gpu_load_apply_ops(self._h, n, _dptr(amps), ctypes.cast(arr, ctypes.c_void_p), len(ops)))
 
     def pass_mark(self) -> int:
         seg = ctypes.c_uint64()

@@ -348,6 +348,11 @@ struct Planner {
 	void *mirror = nullptr;        // a radix pass launched by the next flush also writes its result here
 	bool mirrored = false;         // ... and did
 	const tmfqs_op *base = nullptr;  // the apply_ops call's op array (pass-log op indexes)
+	// Dry run (tmfqs_gpu_load_apply_ops): the first flushed pass is recorded,
+	// not launched.
+	bool dry = false, dry_done = false;
+	size_t dry_ops = 0;
+	tqb::FusedPass dry_pass;
 
 	explicit Planner(tmfqs_gpu_state *hh) : h(hh) {
 		// Tiles of 2^12 complex128 / 2^13 complex64 amplitudes (64 KB).  The
@@ -454,7 +459,10 @@ struct Planner {
 			h->cur_first = (uint64_t)(pending.front() - base);
 			h->cur_count = (unsigned)pending.size();
 		}
-		if(pending.size() == 1) {
+		if(dry && pending.size() == 1) {
+			dry_done = true;  // a single-gate pass: nothing to overlap with
+			dry_ops = 0;
+		} else if(pending.size() == 1) {
 			run_single(*pending[0]);
 		} else {
 			finalize_local_set();
@@ -475,6 +483,12 @@ struct Planner {
 				}
 			}
 			pass.gate_count = (unsigned)pending.size();
+			if(dry) {
+				dry_done = true;
+				dry_ops = pending.size();
+				dry_pass = pass;
+				return;
+			}
 			++npass;
 			PassTimer timer(h, TMFQS_KT_FUSED, sweep_bytes(h));
 			const bool qft = twiddle && h->opt_radix && h->opt_qft_pass &&
@@ -1150,6 +1164,108 @@ bool apply_ops_body(tmfqs_gpu_state *h, const tmfqs_op *ops, size_t count, bool 
 	return p.mirrored;
 }
 
+// tmfqs_gpu_load_apply_ops: loadAmplitudes followed by a batch, with the
+// host-to-device copy overlapped with the batch's first pass.  The first pass
+// is formed as the planner would form it (a dry run); when it is an exact
+// complex128 fused pass whose top four outer bits are consecutive, the state
+// is copied in 16 slabs -- the slab of value v holds the amplitudes whose top
+// outer bits are v: rows of 2^p contiguous amplitudes, one per value of the
+// bits above them (one cudaMemcpy2DAsync) -- on a copy stream, and the pass
+// runs each slab's tiles as soon as that slab has landed.  The rest of the
+// batch runs as tmfqs_gpu_apply_ops.  Anything else (other forms, an invalid
+// op, a batch that does not start with a fused pass) takes the plain path:
+// load, then apply -- with the same results and errors.
+void load_apply_ops_body(tmfqs_gpu_state *h, unsigned n, const double *host, const tmfqs_op *ops, size_t count) {
+	require_handle(h);
+	if(!host) fail(TMFQS_ERR_INVALID_ARGUMENT, "null amplitude buffer");
+	if(count && !ops) fail(TMFQS_ERR_INVALID_ARGUMENT, "null op list");
+	DeviceScope d(h);
+	auto plain = [&] {
+		ensure_state(h, n);
+		h->cache.clear();
+		h->dirty.clear();
+		copy_in(h, 0, host, h->N);
+		h->initialized = true;
+		apply_ops_body(h, ops, count);
+	};
+	if(h->precision != TMFQS_FP64 || !h->opt_exact || !h->opt_fusion || count < 2) return plain();
+	ensure_state(h, n);
+	h->cache.clear();
+	h->dirty.clear();
+	h->initialized = false;
+	try {
+		for(size_t i = 0; i < count; ++i) validate_op(h, ops[i]);
+	} catch(const tqb::Error &) {
+		return plain();  // the plain path applies the ops before the invalid one, then reports it
+	}
+	Planner p(h);
+	p.dry = true;
+	for(size_t i = 0; i < count && !p.dry_done; ++i) {
+		const tmfqs_op &op = ops[i];
+		if(op.kind != TMFQS_OP_H && op.kind != TMFQS_OP_X && op.kind != TMFQS_OP_CNOT && op.kind != TMFQS_OP_CPHASE &&
+		   op.kind != TMFQS_OP_PHASE_FLIP)
+			break;
+		p.add(op);
+	}
+	if(!p.dry_done) p.flush();
+	const size_t k = p.dry_ops;
+	tqb::FusedPass fp = p.dry_pass;
+	// The pass's outer bits, ascending (tile index bit i is outer bit i).
+	std::vector<unsigned> outer;
+	for(unsigned b = 0; b < n; ++b)
+		if(std::find(fp.lpos, fp.lpos + fp.K, b) == fp.lpos + fp.K) outer.push_back(b);
+	constexpr unsigned t = 4;
+	const unsigned nout = (unsigned)outer.size();
+	if(k < 2 || nout < t + 1 || outer[nout - 1] - outer[nout - t] != t - 1) {
+		h->initialized = true;  // state allocated; plain() loads it
+		return plain();
+	}
+	const unsigned pbit = outer[nout - t];
+	if(!h->copy_stream) check_cuda(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking), "copy stream");
+	const size_t width = (size_t(16) << pbit), pitch = (size_t(16) << (pbit + t)), height = size_t(1) << (n - pbit - t);
+	const unsigned slabs = 1u << t;
+	std::vector<cudaEvent_t> ev(slabs, nullptr);
+	struct Events {
+		std::vector<cudaEvent_t> &e;
+		~Events() {
+			for(cudaEvent_t x : e)
+				if(x) cudaEventDestroy(x);
+		}
+	} events{ev};
+	// The copy stream must not overwrite the state while earlier work on the handle's stream still reads it.
+	cudaEvent_t ready = nullptr;
+	check_cuda(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
+	check_cuda(cudaEventRecord(ready, h->stream), "event record");
+	check_cuda(cudaStreamWaitEvent(h->copy_stream, ready, 0), "copy stream wait");
+	cudaEventDestroy(ready);
+	h->initialized = true;
+	h->cur_first = 0;
+	h->cur_count = (unsigned)k;
+	const uint64_t per = (1ull << (nout - t));
+	for(unsigned v = 0; v < slabs; ++v) {
+		unsigned char *dst = static_cast<unsigned char *>(h->amps) + (size_t(v) << pbit) * 16;
+		const unsigned char *src = reinterpret_cast<const unsigned char *>(host) + (size_t(v) << pbit) * 16;
+		check_cuda(cudaMemcpy2DAsync(dst, pitch, src, pitch, width, height, cudaMemcpyHostToDevice, h->copy_stream),
+		           "slab copy");
+		check_cuda(cudaEventCreateWithFlags(&ev[v], cudaEventDisableTiming), "event");
+		check_cuda(cudaEventRecord(ev[v], h->copy_stream), "event record");
+		check_cuda(cudaStreamWaitEvent(h->stream, ev[v], 0), "slab wait");
+		fp.tile_begin = v * per;
+		fp.tile_end = (v + 1) * per;
+		PassTimer timer(h, TMFQS_KT_FUSED, sweep_bytes(h) / slabs);
+		tqb::launch_fused_pass(ctx(h), h->precision, h->amps, fp, h->dev_prog, h->dev_prog_bytes);
+	}
+	h->stats.h2d_bytes += h->N * 16;
+	++h->stats.fused_passes;
+	h->cur_count = 0;
+	if(k < count) {
+		apply_ops_body(h, ops + k, count - k);
+	} else {
+		check_cuda(cudaStreamSynchronize(h->stream), "load_apply_ops sync");
+		check_device_error(h);
+	}
+}
+
 // ---- adjoint gradient (tmfqs_gpu_adjoint_gradient) ----
 // A work handle of `h` (kept in *w between calls) with h's options and a state
 // of h->n qubits; without a state buffer of its own when `with_state` is false
@@ -1514,6 +1630,10 @@ int tmfqs_gpu_destroy(tmfqs_gpu_state *h) {
 		for(unsigned k = 0; k < tqb::UploadRing::kSlots; ++k)
 			if(h->ring.ev[k]) cudaEventDestroy(h->ring.ev[k]);
 		if(h->ring.host) cudaFreeHost(h->ring.host);
+		if(h->copy_stream) {
+			cudaStreamSynchronize(h->copy_stream);
+			cudaStreamDestroy(h->copy_stream);
+		}
 		if(h->stream) cudaStreamDestroy(h->stream);
 		delete h;
 	});
@@ -1884,6 +2004,10 @@ int tmfqs_gpu_gate(tmfqs_gpu_state *h, const double *matrix, const unsigned *qub
 		before_mutation(h);
 		run_gate(h, matrix, qubits, k);
 	});
+}
+
+int tmfqs_gpu_load_apply_ops(tmfqs_gpu_state *h, unsigned n, const double *host, const tmfqs_op *ops, size_t count) {
+	return guarded([&] { load_apply_ops_body(h, n, host, ops, count); });
 }
 
 int tmfqs_debug_fail_allocations(unsigned skip, unsigned count) {

@@ -38,6 +38,7 @@ struct FusedGeom {
 	uint64_t ntiles;
 	unsigned nops;
 	unsigned sw;               // shared-memory swizzle: slot of local index j is j ^ ((j >> sw) & 7)
+	uint64_t o_begin;          // the launch runs tiles [o_begin, ntiles)
 	double inv;                // 1.0 / std::sqrt(2.0), formed on the host (dense_state_backend.cpp:258)
 };
 
@@ -165,7 +166,7 @@ __global__ void __launch_bounds__(kFusedThreads, 3) k_fused(typename Vec2<R>::ty
 	auto P = [&](unsigned j) -> unsigned { return j ^ ((j >> g.sw) & 7u); };
 	const unsigned half = T >> 1, quarter = T >> 2;
 	const R inv = (R)g.inv;
-	for(uint64_t o = blockIdx.x; o < g.ntiles; o += gridDim.x) {
+	for(uint64_t o = g.o_begin + blockIdx.x; o < g.ntiles; o += gridDim.x) {
 		const uint64_t base = expand_outer(o, g);
 		for(unsigned j = threadIdx.x; j < T; j += blockDim.x) s[P(j)] = a[base | scatter(j)];
 		__syncthreads();
@@ -796,6 +797,12 @@ void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	if(g.m == 0 || pass.K > kMaxLocal) fail(TMFQS_ERR_LOGIC, "fused pass: bad local set");
 	for(unsigned i = 0; i < pass.K; ++i) g.lpos[i] = pass.lpos[i];
 	g.ntiles = 1ull << (pass.n - pass.K);
+	g.o_begin = 0;
+	if(pass.tile_end) {
+		if(pass.tile_begin >= pass.tile_end || pass.tile_end > g.ntiles) fail(TMFQS_ERR_LOGIC, "fused pass: bad tile range");
+		g.o_begin = pass.tile_begin;
+		g.ntiles = pass.tile_end;
+	}
 	g.nops = (unsigned)pass.ops.size();
 	g.inv = 1.0 / std::sqrt(2.0);
 	// Tiles of >= 7 local bits: swizzled shared memory and per-chain thread layouts.
@@ -840,7 +847,7 @@ void run_fused(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_pr
 	check_cuda(cudaFuncSetAttribute(k_fused<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fused smem");
 	int per_sm = 1;
 	check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused<R>, kFusedThreads, smem), "fused occupancy");
-	const uint64_t grid = std::min<uint64_t>(g.ntiles, (uint64_t)c.num_sms * std::max(1, per_sm));
+	const uint64_t grid = std::min<uint64_t>(g.ntiles - g.o_begin, (uint64_t)c.num_sms * std::max(1, per_sm));
 	k_fused<R><<<(unsigned)grid, kFusedThreads, smem, c.stream>>>(
 		static_cast<typename Vec2<R>::type *>(a), g, static_cast<const FusedOp *>(dev_prog),
 		reinterpret_cast<const ChainEntry *>(static_cast<unsigned char *>(dev_prog) + ph_off),

@@ -164,6 +164,8 @@ struct FusedPass {
 	std::vector<FusedOp> ops;
 	std::vector<ChainEntry> chain;  // H-chain entries of all chains of the pass
 	unsigned gate_count = 0;        // circuit operations folded into this pass
+	// Exact fused passes: run only tiles [tile_begin, tile_end) (0, 0: all).
+	uint64_t tile_begin = 0, tile_end = 0;
 };
 
 // Runs one fused pass over the whole state.  `dev_prog` is a device buffer
@@ -276,6 +278,7 @@ struct tmfqs_gpu_state {
 	void *amps = nullptr;
 	size_t bytes = 0;
 	cudaStream_t stream = nullptr;
+	cudaStream_t copy_stream = nullptr;  // tmfqs_gpu_load_apply_ops: host-to-device slabs
 	tqb::SeqScratch seq;
 	// Host cache of single amplitudes (amplitude / setAmplitude / phase flips
 	// of cached states); dirty entries are flushed before any kernel runs.
