@@ -58,47 +58,39 @@ struct ChainMap {
 	uint64_t mr[128];  // per warp-iteration q: the same for its offset
 	uint16_t jl[32];   // per lane: local index offset
 	uint16_t jr[128];  // per q: local index offset
-	uint32_t nq;       // number of q values, 2^(K-6)
-	uint32_t ilp;      // 1: bit 0 of q is no control, so q and q+1 share their mask
-	uint32_t pad[2];
+	uint64_t mall;     // the union of ml over the lanes
+	uint32_t nq;       // number of q values, 2^(K-6); a thread takes kChainPairs consecutive q together
+	uint32_t ilp;      // the low bits of q that are no control (their pairs share a mask): 0, 1 or 2
+	uint32_t narrow;   // the chain has at most 32 entries: masks live in their high word
+	uint32_t pad;
 };
 constexpr uint64_t kNoChainMap = ~0ull;
 
-// Applies the chain entries of mask m (entry e = bit 63-e, ascending e =
-// circuit order) to one amplitude: each a separately rounded complex product
-// (dense_state_backend.cpp:300-301), exactly as the per-gate path.
-template <typename R>
-__device__ __forceinline__ void chain_apply(uint64_t m, const double2 *cph, R &r, R &i) {
-	for(uint32_t hi = (uint32_t)(m >> 32); hi;) {
-		const unsigned e = __clz(hi);
-		hi ^= 0x80000000u >> e;
-		const double2 ph = cph[e];
-		cmul_ref((R)ph.x, (R)ph.y, r, i);
-	}
-	for(uint32_t lo = (uint32_t)m; lo;) {
-		const unsigned e = __clz(lo);
-		lo ^= 0x80000000u >> e;
-		const double2 ph = cph[32 + e];
-		cmul_ref((R)ph.x, (R)ph.y, r, i);
-	}
-}
+#ifndef TMFQS_CHAIN_PAIRS
+#define TMFQS_CHAIN_PAIRS 4
+#endif
+// Butterflies per thread in a mapped H-chain op: independent chains of
+// dependent products that hide each other's latency.
+constexpr unsigned kChainPairs = TMFQS_CHAIN_PAIRS;
 
-// The same for two amplitudes with the same mask.
-template <typename R>
-__device__ __forceinline__ void chain_apply2(uint64_t m, const double2 *cph, R &ra, R &ia, R &rb, R &ib) {
-	for(uint32_t hi = (uint32_t)(m >> 32); hi;) {
-		const unsigned e = __clz(hi);
-		hi ^= 0x80000000u >> e;
+// Chain products over one 32-entry word of a warp-uniform mask `mw` (the
+// union of the masks of all lanes and pairs; entry e = bit 31 - e of the
+// word, ascending e = circuit order): every lane walks the same entries, reads
+// each phase once (a shared-memory broadcast), and applies it to each of its
+// amplitudes whose own mask has it -- a separately rounded complex product
+// (dense_state_backend.cpp:300-301), exactly as the per-gate path.
+template <typename R, unsigned NP>
+__device__ __forceinline__ void chain_word(uint32_t mw, const uint32_t (&mk)[NP], const double2 *cph, R (&r)[NP],
+                                           R (&i)[NP]) {
+	while(mw) {
+		const unsigned e = __clz(mw);
+		const uint32_t bit = 0x80000000u >> e;
+		mw ^= bit;
 		const double2 ph = cph[e];
-		cmul_ref((R)ph.x, (R)ph.y, ra, ia);
-		cmul_ref((R)ph.x, (R)ph.y, rb, ib);
-	}
-	for(uint32_t lo = (uint32_t)m; lo;) {
-		const unsigned e = __clz(lo);
-		lo ^= 0x80000000u >> e;
-		const double2 ph = cph[32 + e];
-		cmul_ref((R)ph.x, (R)ph.y, ra, ia);
-		cmul_ref((R)ph.x, (R)ph.y, rb, ib);
+		const R pr = (R)ph.x, pi = (R)ph.y;
+#pragma unroll
+		for(unsigned k = 0; k < NP; ++k)
+			if(mk[k] & bit) cmul_ref(pr, pi, r[k], i[k]);
 	}
 }
 
@@ -126,8 +118,11 @@ __device__ __forceinline__ bool butterfly(typename Vec2<R>::type &x, typename Ve
 	return true;
 }
 
+#ifndef TMFQS_FUSED_MIN_BLOCKS
+#define TMFQS_FUSED_MIN_BLOCKS 3
+#endif
 template <typename R>
-__global__ void __launch_bounds__(kFusedThreads, 3) k_fused(typename Vec2<R>::type *a, FusedGeom g, const FusedOp *ops,
+__global__ void __launch_bounds__(kFusedThreads, TMFQS_FUSED_MIN_BLOCKS) k_fused(typename Vec2<R>::type *a, FusedGeom g, const FusedOp *ops,
                                                             const ChainEntry *chain, const ChainMap *maps) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ unsigned char smem_raw[];
@@ -142,6 +137,9 @@ __global__ void __launch_bounds__(kFusedThreads, 3) k_fused(typename Vec2<R>::ty
 	__shared__ int cloc[64];
 	__shared__ unsigned ccount;
 	__shared__ uint64_t cu;  // mapped chains: entries whose control is an outer bit set in this tile
+	// The current chain op's thread layout, staged from the program (tile-independent).
+	__shared__ uint64_t sml[32], smr[128];
+	__shared__ uint16_t sjl[32], sjr[128];
 	// Twiddle form: table A (outer phase x first 6 local controls) and table B
 	// (next 5 local controls), built per tile in FP64.
 	__shared__ double2 twa[64], twb[32];
@@ -202,56 +200,65 @@ __global__ void __launch_bounds__(kFusedThreads, 3) k_fused(typename Vec2<R>::ty
 								u |= (uint64_t)__brev(b) << (e0 == 0 ? 32 : 0);
 							}
 							if(lane == 0) cu = u;
+						} else {
+							// The other warps stage the op's layout in shared memory.
+							const ChainMap &gm = maps[op.state];
+							for(unsigned k = threadIdx.x - 32; k < gm.nq; k += blockDim.x - 32) {
+								smr[k] = gm.mr[k];
+								sjr[k] = gm.jr[k];
+							}
+							if(threadIdx.x < 64) {
+								sml[threadIdx.x - 32] = gm.ml[threadIdx.x - 32];
+								sjl[threadIdx.x - 32] = gm.jl[threadIdx.x - 32];
+							}
 						}
 						__syncthreads();
 						const ChainMap &cm = maps[op.state];
-						const unsigned tb = 1u << op.lt, jl = cm.jl[lane];
-						const uint64_t mlane = cm.ml[lane] | cu;
+						const unsigned tb = 1u << op.lt, jl = sjl[lane];
+						const uint64_t mlane = sml[lane] | cu;
 						const unsigned warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-						if(cm.ilp) {
-							// Two butterflies per thread whose |1> outputs take the same
-							// phases (they differ in a bit that is no control).
-							for(unsigned q = 2 * warp; q < cm.nq; q += 2 * nw) {
-								const unsigned ja = jl | cm.jr[q], jb = jl | cm.jr[q + 1];
-								const uint64_t m = mlane | cm.mr[q];
-								V xa = s[P(ja)], ya = s[P(ja | tb)], xb = s[P(jb)], yb = s[P(jb | tb)];
-								const bool wa = butterfly<R>(xa, ya, inv), wb = butterfly<R>(xb, yb, inv);
-								// A zero |1> output is left alone by every phase (dense_state_backend.cpp:299).
-								const bool ca = wa && !is_zero<R>(ya), cb = wb && !is_zero<R>(yb);
-								if(ca || cb) {
-									R ra = ya.x, ia = ya.y, rb = yb.x, ib = yb.y;
-									chain_apply2<R>(m, cph, ra, ia, rb, ib);
-									if(ca) {
-										ya.x = ra;
-										ya.y = ia;
-									}
-									if(cb) {
-										yb.x = rb;
-										yb.y = ib;
-									}
-								}
-								if(wa) {
-									s[P(ja)] = xa;
-									s[P(ja | tb)] = ya;
-								}
-								if(wb) {
-									s[P(jb)] = xb;
-									s[P(jb | tb)] = yb;
-								}
+						// Two butterflies per thread (q and q+1): two independent chains
+						// of dependent products.  Their |1> outputs share one mask when the
+						// bit they differ in is no control.
+						const unsigned nq = cm.nq;
+						const bool narrow = cm.narrow != 0;
+						const uint64_t mall = cm.mall | cu;  // the entries any lane of a warp can need
+						constexpr unsigned NP = kChainPairs;
+						for(unsigned q0 = NP * warp; q0 < nq; q0 += NP * nw) {
+							unsigned jk[NP];
+							uint64_t mk[NP];
+							V x[NP], y[NP];
+							bool w[NP];
+							uint64_t mw = mall;
+#pragma unroll
+							for(unsigned k = 0; k < NP; ++k) {
+								jk[k] = jl | sjr[q0 + k];
+								mk[k] = mlane | smr[q0 + k];
+								mw |= smr[q0 + k];
+								x[k] = s[P(jk[k])];
+								y[k] = s[P(jk[k] | tb)];
+								w[k] = butterfly<R>(x[k], y[k], inv);
 							}
-						} else {
-							for(unsigned q = warp; q < cm.nq; q += nw) {
-								const unsigned ja = jl | cm.jr[q];
-								V x = s[P(ja)], y = s[P(ja | tb)];
-								if(!butterfly<R>(x, y, inv)) continue;
-								if(!is_zero<R>(y)) {
-									R r = y.x, i = y.y;
-									chain_apply<R>(mlane | cm.mr[q], cph, r, i);
-									y.x = r;
-									y.y = i;
-								}
-								s[P(ja)] = x;
-								s[P(ja | tb)] = y;
+							R r[NP], im[NP];
+							uint32_t hi[NP], lo[NP];
+#pragma unroll
+							for(unsigned k = 0; k < NP; ++k) {
+								// A zero |1> output is left alone by every phase (dense_state_backend.cpp:299).
+								const bool c = w[k] && !is_zero<R>(y[k]);
+								hi[k] = c ? (uint32_t)(mk[k] >> 32) : 0u;
+								lo[k] = c ? (uint32_t)mk[k] : 0u;
+								r[k] = y[k].x;
+								im[k] = y[k].y;
+							}
+							chain_word<R, NP>((uint32_t)(mw >> 32), hi, cph, r, im);
+							if(!narrow) chain_word<R, NP>((uint32_t)mw, lo, cph + 32, r, im);
+#pragma unroll
+							for(unsigned k = 0; k < NP; ++k) {
+								if(!w[k]) continue;
+								y[k].x = r[k];
+								y[k].y = im[k];
+								s[P(jk[k])] = x[k];
+								s[P(jk[k] | tb)] = y[k];
 							}
 						}
 						__syncthreads();
@@ -757,13 +764,20 @@ ChainMap build_chain_map(const FusedPass &pass, const FusedOp &op) {
 		if(b < 0) b = next(false);
 		take((unsigned)b);
 	}
-	const int ilp = next(true);
-	if(ilp >= 0) take((unsigned)ilp);
+	// Bits 0 and 1 of q: the bits a thread's butterflies differ in (free ones first).
+	unsigned nfree = 0;
+	for(unsigned i = 0; i < 2 && order.size() < K - 1; ++i) {
+		int b = next(true);
+		if(b >= 0 && nfree == i) ++nfree;
+		if(b < 0) b = next(false);
+		take((unsigned)b);
+	}
 	for(int b = next(false); b >= 0; b = next(false)) take((unsigned)b);
 	if(order.size() != K - 1) fail(TMFQS_ERR_LOGIC, "fused pass: chain layout");
 	ChainMap m{};
 	m.nq = 1u << (K - 6);
-	m.ilp = ilp >= 0 ? 1u : 0u;
+	m.ilp = nfree;
+	m.narrow = op.lc <= 32 ? 1u : 0u;
 	auto mask_of = [&](unsigned j) {
 		uint64_t r = 0;
 		for(const auto &pe : loc)
@@ -776,6 +790,7 @@ ChainMap build_chain_map(const FusedPass &pass, const FusedOp &op) {
 			if((l >> i) & 1u) j |= 1u << order[i];
 		m.jl[l] = (uint16_t)j;
 		m.ml[l] = mask_of(j);
+		m.mall |= m.ml[l];
 	}
 	for(unsigned q = 0; q < m.nq; ++q) {
 		unsigned j = 0;
@@ -934,12 +949,444 @@ void run_perm(const LaunchCtx &c, void *a, unsigned n, const std::vector<std::pa
 	after_launch(c, "bit permutation");
 }
 
+// ---------------------------------------------------------------------------
+// Register stages for exact passes of Hadamards and H-chains (the QFT).
+//
+// A pass's ops are cut into stages of up to four consecutive Hadamard
+// targets.  In a stage every thread holds the 16 amplitudes of the tile that
+// differ only in the stage's four register bits and applies the stage's ops
+// to them in circuit order, in registers: each Hadamard as 8 butterflies, each
+// of its chain's controlled phases as separately rounded complex products on
+// the |1> outputs whose control bit is set -- the same IEEE operations, in the
+// same order per amplitude, as the per-gate path (dense_state_backend.cpp:
+// 255-304), so the result is bit-identical.  A stage reads and writes the tile
+// in shared memory once and takes one barrier (instead of one of each per
+// op), and each Hadamard's 8 |1> outputs are 8 independent chains of dependent
+// products per thread.  The controls of a chain entry are an outer bit (set or
+// not for the whole tile), a local bit that indexes the thread (set or not
+// for the thread), or a register bit (set for half of the thread's outputs).
+// Lanes walk the entries of the warp's union mask together (one broadcast
+// phase load per entry); each output applies those in its own mask.
+// ---------------------------------------------------------------------------
+constexpr unsigned kStRB = 4;               // register bits per stage
+constexpr unsigned kStK = 12;               // local bits of a tile (complex128: 64 KiB)
+constexpr unsigned kStThreads = 1u << (kStK - kStRB);
+constexpr unsigned kStMaxOps = 16;
+constexpr unsigned kStMaxStages = 8;
+constexpr unsigned kStMaxEntries = 1024;
+
+struct StageGeom {
+	unsigned n, m;
+	unsigned lpos[kStK];
+	uint64_t ntiles, o_begin;
+	unsigned nops, nstages, nentries, narrow;
+	double inv;
+	uint8_t st_first[kStMaxStages], st_count[kStMaxStages];
+	uint8_t rbit[kStMaxStages][kStRB];        // local bit of register bit i
+	uint8_t tbit[kStMaxStages][kStK - kStRB];  // local bit of thread index bit k
+	uint16_t tlo[kStMaxStages][16], thi[kStMaxStages][16];  // thread index nibbles -> local offset
+	uint8_t op_reg[kStMaxOps];                 // register bit of the op's Hadamard
+	uint16_t op_tab[kStMaxOps], op_lc[kStMaxOps];  // its chain: entries [tab, tab + lc) of the pass
+	uint8_t swz[3];                            // slot bit i ^= index bit swz[i] (0: none)
+};
+
+// Shared slot of local index j: bits 0-2 XORed with three higher bits chosen
+// per pass (stage_swizzle) so that each stage's quarter-warps read 8 distinct
+// 16-byte bank groups.  XOR-linear: slot(a ^ b) = slot(a) ^ slot(b).
+__device__ __forceinline__ unsigned st_slot(unsigned j, const uint8_t (&swz)[3]) {
+	unsigned x = j;
+#pragma unroll
+	for(unsigned i = 0; i < 3; ++i)
+		if(swz[i]) x ^= ((j >> swz[i]) & 1u) << i;
+	return x;
+}
+
+// The |1> output p (of the 8 of a Hadamard on register bit I) is register r1(p).
+template <unsigned I>
+__device__ __forceinline__ constexpr unsigned st_r1(unsigned p) {
+	return ((p >> I) << (I + 1)) | (p & ((1u << I) - 1u)) | (1u << I);
+}
+
+// One rounded complex product (dense_state_backend.cpp:300-301) on output p
+// when `on`: computed unconditionally and kept by a select, so that the
+// products of independent outputs interleave (a skipped product leaves the
+// value exactly as it was).  ALLNZ: every output is nonzero (the common case).
+template <typename R, bool ALLNZ>
+__device__ __forceinline__ void st_cmul(R pr, R pi, typename Vec2<R>::type &x, bool on) {
+	R re = x.x, im = x.y;
+	cmul_ref(pr, pi, re, im);
+	if(ALLNZ) {
+		x.x = re;
+		x.y = im;
+	} else {
+		x.x = on ? re : x.x;
+		x.y = on ? im : x.y;
+	}
+}
+
+// Products of one entry whose control is register bit J: the 4 outputs with
+// bit J set (a compile-time subset).
+template <typename R, unsigned I, unsigned J, bool ALLNZ>
+__device__ __forceinline__ void st_apply_reg(R pr, R pi, const bool (&nz)[8], typename Vec2<R>::type (&v)[16]) {
+#pragma unroll
+	for(unsigned p = 0; p < 8; ++p)
+		if((st_r1<I>(p) >> J) & 1u) st_cmul<R, ALLNZ>(pr, pi, v[st_r1<I>(p)], nz[p]);
+}
+
+// Walks one 32-entry word W (H: high word of the masks, else low) of the
+// warp's union of entries in circuit order.  An entry controlled by a
+// register bit goes to the outputs with that bit set; any other entry (an
+// outer bit or a thread bit: the same for all of this thread's outputs) to all
+// 8 when the thread's mask tw has it.  Zero outputs are skipped (nz).
+template <typename R, unsigned I, int W, bool ALLNZ>
+__device__ __forceinline__ void stage_walk(uint32_t tw, const uint64_t (&rm)[kStRB], uint32_t w, const double2 *cph,
+                                           const bool (&nz)[8], typename Vec2<R>::type (&v)[16]) {
+	const uint32_t r0 = W ? (uint32_t)rm[0] : (uint32_t)(rm[0] >> 32), r1 = W ? (uint32_t)rm[1] : (uint32_t)(rm[1] >> 32);
+	const uint32_t r2 = W ? (uint32_t)rm[2] : (uint32_t)(rm[2] >> 32), r3 = W ? (uint32_t)rm[3] : (uint32_t)(rm[3] >> 32);
+	while(w) {
+		const unsigned e = __clz(w);
+		const uint32_t bit = 0x80000000u >> e;
+		w ^= bit;
+		const double2 c = cph[e];
+		const R pr = (R)c.x, pi = (R)c.y;
+		if(r0 & bit) {
+			if constexpr(I != 0) st_apply_reg<R, I, 0, ALLNZ>(pr, pi, nz, v);
+		} else if(r1 & bit) {
+			if constexpr(I != 1) st_apply_reg<R, I, 1, ALLNZ>(pr, pi, nz, v);
+		} else if(r2 & bit) {
+			if constexpr(I != 2) st_apply_reg<R, I, 2, ALLNZ>(pr, pi, nz, v);
+		} else if(r3 & bit) {
+			if constexpr(I != 3) st_apply_reg<R, I, 3, ALLNZ>(pr, pi, nz, v);
+		} else if(tw & bit) {
+#pragma unroll
+			for(unsigned p = 0; p < 8; ++p) st_cmul<R, ALLNZ>(pr, pi, v[st_r1<I>(p)], nz[p]);
+		}
+	}
+}
+
+template <typename R, unsigned I, bool NARROW>
+__device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R inv, bool chain, unsigned st, unsigned k,
+                                             const StageGeom &g, const uint64_t *lb, const double2 *ph, uint64_t cu,
+                                             unsigned t) {
+	typedef typename Vec2<R>::type V;
+	bool nz[8];
+#pragma unroll
+	for(unsigned p = 0; p < 8; ++p) {
+		const unsigned r0 = ((p >> I) << (I + 1)) | (p & ((1u << I) - 1u)), r1 = r0 | (1u << I);
+		nz[p] = butterfly<R>(v[r0], v[r1], inv) && !is_zero<R>(v[r1]);
+	}
+	if(!chain) return;
+	const uint64_t *L = lb + (size_t)k * kStK;
+	// Entries whose control is fixed for this thread: outer bits of the tile, the thread's local bits.
+	uint64_t tm = cu;
+#pragma unroll
+	for(unsigned b = 0; b < kStK - kStRB; ++b)
+		if((t >> b) & 1u) tm |= L[g.tbit[st][b]];
+	uint64_t rm[kStRB];
+	uint64_t un = tm;
+#pragma unroll
+	for(unsigned j = 0; j < kStRB; ++j) {
+		rm[j] = j == I ? 0ull : L[g.rbit[st][j]];
+		un |= rm[j];
+	}
+	const double2 *cph = ph + g.op_tab[k];
+	// The union over the warp's lanes: every lane walks the same entries.
+	const uint32_t wh = __reduce_or_sync(0xffffffffu, (uint32_t)(un >> 32));
+	const uint32_t wl = NARROW ? 0u : __reduce_or_sync(0xffffffffu, (uint32_t)un);
+	bool all = true;
+#pragma unroll
+	for(unsigned p = 0; p < 8; ++p) all = all && nz[p];
+	if(all) {
+		stage_walk<R, I, 0, true>((uint32_t)(tm >> 32), rm, wh, cph, nz, v);
+		if constexpr(!NARROW) stage_walk<R, I, 1, true>((uint32_t)tm, rm, wl, cph + 32, nz, v);
+	} else {
+		stage_walk<R, I, 0, false>((uint32_t)(tm >> 32), rm, wh, cph, nz, v);
+		if constexpr(!NARROW) stage_walk<R, I, 1, false>((uint32_t)tm, rm, wl, cph + 32, nz, v);
+	}
+}
+
+template <typename R, bool NARROW>
+__global__ void __launch_bounds__(kStThreads, 2) k_fused_stages(typename Vec2<R>::type *a, const __grid_constant__ StageGeom g,
+                                                                const FusedOp *ops, const ChainEntry *chain,
+                                                                const double2 *gph, const uint64_t *glb) {
+	typedef typename Vec2<R>::type V;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	constexpr unsigned T = 1u << kStK;
+	const unsigned nhi = 1u << (kStK - g.m);
+	// Regions at 16-byte boundaries (the phases are read as 16-byte values).
+	auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+	V *s = reinterpret_cast<V *>(smem_raw);
+	const size_t o_hi = sizeof(V) * T, o_lb = o_hi + a16(sizeof(uint64_t) * nhi);
+	const size_t o_ph = o_lb + a16(sizeof(uint64_t) * g.nops * kStK), o_cu = o_ph + sizeof(double2) * g.nentries;
+	const size_t o_eb = o_cu + sizeof(uint64_t) * g.nops;
+	uint64_t *hitab = reinterpret_cast<uint64_t *>(smem_raw + o_hi);
+	uint64_t *lb = reinterpret_cast<uint64_t *>(smem_raw + o_lb);
+	double2 *ph = reinterpret_cast<double2 *>(smem_raw + o_ph);
+	uint64_t *cus = reinterpret_cast<uint64_t *>(smem_raw + o_cu);
+	uint8_t *ebit = smem_raw + o_eb;  // per entry: its outer control bit, or 0xff for a local control
+	const unsigned t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+	for(unsigned h = t; h < nhi; h += blockDim.x) {
+		uint64_t v = 0;
+		for(unsigned i = 0; i < kStK - g.m; ++i)
+			if((h >> i) & 1u) v |= 1ull << g.lpos[g.m + i];
+		hitab[h] = v;
+	}
+	for(unsigned e = t; e < g.nops * kStK; e += blockDim.x) lb[e] = glb[e];
+	for(unsigned e = t; e < g.nentries; e += blockDim.x) ph[e] = gph[e];
+	for(unsigned k = 0; k < g.nops; ++k)
+		for(unsigned e = t; e < g.op_lc[k]; e += blockDim.x) {
+			const ChainEntry ce = chain[g.op_tab[k] + e];
+			ebit[g.op_tab[k] + e] = ce.local < 0 ? (uint8_t)ce.bit : (uint8_t)0xff;
+		}
+	__syncthreads();
+	const unsigned lowmask = (1u << g.m) - 1u;
+	auto scatter = [&](unsigned j) -> uint64_t { return (uint64_t)(j & lowmask) | hitab[j >> g.m]; };
+	const R inv = (R)g.inv;
+	for(uint64_t o = g.o_begin + blockIdx.x; o < g.ntiles; o += gridDim.x) {
+		uint64_t base = o;
+		for(unsigned i = 0; i < kStK; ++i) base = insert0(base, g.lpos[i]);
+		for(unsigned j = t; j < T; j += blockDim.x) s[st_slot(j, g.swz)] = a[base | scatter(j)];
+		// The chain entries whose control is an outer bit set in this tile: one
+		// warp per op, one lane per entry (entry e = bit 63 - e).
+		for(unsigned k = warp; k < g.nops; k += blockDim.x >> 5) {
+			uint64_t u = 0;
+			for(unsigned e0 = 0; e0 < g.op_lc[k]; e0 += 32) {
+				const unsigned e = e0 + lane;
+				const unsigned b = e < g.op_lc[k] ? ebit[g.op_tab[k] + e] : 0xffu;
+				const unsigned on = __ballot_sync(0xffffffffu, b != 0xffu && ((base >> b) & 1ull));
+				u |= (uint64_t)__brev(on) << (e0 == 0 ? 32 : 0);
+			}
+			if(lane == 0) cus[k] = u;
+		}
+		__syncthreads();
+		for(unsigned st = 0; st < g.nstages; ++st) {
+			const unsigned jb = st_slot((unsigned)g.tlo[st][t & 15u] | g.thi[st][t >> 4], g.swz);
+			unsigned ro[kStRB];
+#pragma unroll
+			for(unsigned i = 0; i < kStRB; ++i) ro[i] = st_slot(1u << g.rbit[st][i], g.swz);
+			unsigned off[16];
+#pragma unroll
+			for(unsigned r = 0; r < 16; ++r) {
+				unsigned x = jb;
+#pragma unroll
+				for(unsigned i = 0; i < kStRB; ++i)
+					if((r >> i) & 1u) x ^= ro[i];
+				off[r] = x;
+			}
+			V v[16];
+#pragma unroll
+			for(unsigned r = 0; r < 16; ++r) v[r] = s[off[r]];
+			const unsigned k1 = g.st_first[st] + g.st_count[st];
+			for(unsigned k = g.st_first[st]; k < k1; ++k) {
+				const bool chain_op = ops[k].kind == kFHChain;
+				const uint64_t cu = cus[k];
+				switch(g.op_reg[k]) {
+					case 0: stage_hchain<R, 0, NARROW>(v, inv, chain_op, st, k, g, lb, ph, cu, t); break;
+					case 1: stage_hchain<R, 1, NARROW>(v, inv, chain_op, st, k, g, lb, ph, cu, t); break;
+					case 2: stage_hchain<R, 2, NARROW>(v, inv, chain_op, st, k, g, lb, ph, cu, t); break;
+					default: stage_hchain<R, 3, NARROW>(v, inv, chain_op, st, k, g, lb, ph, cu, t); break;
+				}
+			}
+#pragma unroll
+			for(unsigned r = 0; r < 16; ++r) s[off[r]] = v[r];
+			__syncthreads();
+		}
+		for(unsigned j = t; j < T; j += blockDim.x) a[base | scatter(j)] = s[st_slot(j, g.swz)];
+		__syncthreads();
+	}
+}
+
+// A swizzle under which every stage's quarter-warp lanes (thread index bits
+// 0-2) move 8 distinct bank groups: over GF(2), the slot bits 0-2 that lane
+// bits flip must be independent.  Searched over three XOR sources.
+void stage_swizzle(StageGeom &g) {
+	auto ok = [&](const uint8_t (&sw)[3]) {
+		for(unsigned st = 0; st < g.nstages; ++st) {
+			unsigned vec[3];
+			for(unsigned l = 0; l < 3; ++l) {
+				const unsigned b = g.tbit[st][l];
+				unsigned v = b < 3 ? (1u << b) : 0u;
+				for(unsigned i = 0; i < 3; ++i)
+					if(sw[i] && sw[i] == b) v ^= 1u << i;
+				vec[l] = v;
+			}
+			// Independent iff no nonempty subset XORs to zero.
+			for(unsigned m = 1; m < 8; ++m) {
+				unsigned x = 0;
+				for(unsigned l = 0; l < 3; ++l)
+					if((m >> l) & 1u) x ^= vec[l];
+				if(!x) return false;
+			}
+		}
+		return true;
+	};
+	uint8_t sw[3] = {0, 0, 0};
+	if(ok(sw)) {
+		std::memcpy(g.swz, sw, 3);
+		return;
+	}
+	for(unsigned a = 0; a < kStK; ++a)
+		for(unsigned b = 0; b < kStK; ++b)
+			for(unsigned c = 0; c < kStK; ++c) {
+				const unsigned v[3] = {a, b, c};
+				bool valid = true;
+				for(unsigned i = 0; i < 3; ++i) valid = valid && (v[i] == 0 || v[i] >= 3);
+				if(!valid) continue;
+				uint8_t t3[3] = {(uint8_t)a, (uint8_t)b, (uint8_t)c};
+				if(ok(t3)) {
+					std::memcpy(g.swz, t3, 3);
+					return;
+				}
+			}
+	std::memset(g.swz, 0, 3);  // none fits every stage: unswizzled (correct, with some conflicts)
+}
+
+// The stage plan of an exact pass, when its program is Hadamards and H-chains
+// on distinct local bits of a 12-bit tile; false otherwise (k_fused runs it).
+bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phases, std::vector<uint64_t> &lbits) {
+	if(pass.K != kStK || pass.ops.empty() || pass.ops.size() > kStMaxOps) return false;
+	g = StageGeom{};
+	g.n = pass.n;
+	g.m = 0;
+	while(g.m < pass.K && pass.lpos[g.m] == g.m) ++g.m;
+	if(g.m == 0) return false;
+	for(unsigned i = 0; i < kStK; ++i) g.lpos[i] = pass.lpos[i];
+	uint32_t seen = 0;
+	unsigned maxlc = 0, nent = 0;
+	for(const FusedOp &op : pass.ops) {
+		if(op.kind != kFH && op.kind != kFHChain) return false;
+		if(op.lt >= kStK || ((seen >> op.lt) & 1u)) return false;
+		seen |= 1u << op.lt;
+		const unsigned lc = op.kind == kFHChain ? op.lc : 0u;
+		if(lc > 64) return false;
+		maxlc = std::max(maxlc, lc);
+		nent += lc;
+	}
+	if(nent > kStMaxEntries) return false;
+	g.nops = (unsigned)pass.ops.size();
+	g.narrow = maxlc <= 32;
+	g.inv = 1.0 / std::sqrt(2.0);
+	// Stages: consecutive ops while their targets fit in four register bits.
+	std::vector<std::vector<unsigned>> regs;
+	for(unsigned k = 0; k < g.nops; ++k) {
+		const unsigned lt = pass.ops[k].lt;
+		if(regs.empty() || regs.back().size() == kStRB) {
+			if(g.nstages == kStMaxStages) return false;
+			regs.push_back({});
+			g.st_first[g.nstages] = (uint8_t)k;
+			++g.nstages;
+		}
+		regs.back().push_back(lt);
+		g.op_reg[k] = (uint8_t)(regs.back().size() - 1);
+		++g.st_count[g.nstages - 1];
+	}
+	for(unsigned st = 0; st < g.nstages; ++st) {
+		std::vector<unsigned> &R = regs[st];
+		// Filler register bits: high local bits first (local bits 0-2 stay thread bits:
+		// a quarter-warp then reads 8 consecutive 16-byte slots, no bank conflict).
+		for(int b = (int)kStK - 1; b >= 0 && R.size() < kStRB; --b)
+			if(std::find(R.begin(), R.end(), (unsigned)b) == R.end()) R.push_back((unsigned)b);
+		uint32_t rset = 0;
+		for(unsigned i = 0; i < kStRB; ++i) {
+			g.rbit[st][i] = (uint8_t)R[i];
+			rset |= 1u << R[i];
+		}
+		unsigned kk = 0;
+		for(unsigned b = 0; b < kStK; ++b)
+			if(!((rset >> b) & 1u)) g.tbit[st][kk++] = (uint8_t)b;
+		for(unsigned x = 0; x < 16; ++x) {
+			unsigned lo = 0, hi = 0;
+			for(unsigned i = 0; i < 4; ++i) {
+				if((x >> i) & 1u) lo |= 1u << g.tbit[st][i];
+				if((x >> i) & 1u) hi |= 1u << g.tbit[st][4 + i];
+			}
+			g.tlo[st][x] = (uint16_t)lo;
+			g.thi[st][x] = (uint16_t)hi;
+		}
+	}
+	phases.clear();
+	lbits.assign((size_t)g.nops * kStK, 0ull);
+	for(unsigned k = 0; k < g.nops; ++k) {
+		const FusedOp &op = pass.ops[k];
+		const unsigned lc = op.kind == kFHChain ? op.lc : 0u;
+		g.op_tab[k] = (uint16_t)phases.size();
+		g.op_lc[k] = (uint16_t)lc;
+		for(unsigned e = 0; e < lc; ++e) {
+			const ChainEntry &ce = pass.chain[op.tab + e];
+			phases.push_back(double2{ce.cr, ce.ci});
+			if(ce.local >= 0) lbits[(size_t)k * kStK + ce.local] |= 1ull << (63 - e);
+		}
+	}
+	g.nentries = (unsigned)phases.size();
+	stage_swizzle(g);
+	return true;
+}
+
+template <typename R>
+bool run_fused_stages(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_prog, size_t &dev_prog_bytes) {
+	StageGeom g;
+	std::vector<double2> phases;
+	std::vector<uint64_t> lbits;
+	if(!plan_stages(pass, g, phases, lbits)) return false;
+	g.ntiles = 1ull << (pass.n - kStK);
+	g.o_begin = 0;
+	if(pass.tile_end) {
+		if(pass.tile_begin >= pass.tile_end || pass.tile_end > g.ntiles) fail(TMFQS_ERR_LOGIC, "fused pass: bad tile range");
+		g.o_begin = pass.tile_begin;
+		g.ntiles = pass.tile_end;
+	}
+	const size_t ops_bytes = pass.ops.size() * sizeof(FusedOp);
+	const size_t ch_off = (ops_bytes + 255) & ~size_t(255);
+	const size_t ch_bytes = std::max<size_t>(32, pass.chain.size() * sizeof(ChainEntry));
+	const size_t ph_off = (ch_off + ch_bytes + 255) & ~size_t(255);
+	const size_t lb_off = (ph_off + std::max<size_t>(16, phases.size() * sizeof(double2)) + 255) & ~size_t(255);
+	const size_t need = lb_off + lbits.size() * sizeof(uint64_t);
+	if(need > dev_prog_bytes) {
+		if(dev_prog) {
+			check_cuda(cudaStreamSynchronize(c.stream), "fused program sync");
+			cudaFree(dev_prog);
+		}
+		dev_prog = nullptr;
+		dev_prog_bytes = 0;
+		if(device_alloc(&dev_prog, need * 2) != cudaSuccess) {
+			cudaGetLastError();
+			fail(TMFQS_ERR_NOMEM, "fused pass program allocation failed");
+		}
+		dev_prog_bytes = need * 2;
+	}
+	std::vector<unsigned char> host(need, 0);
+	std::memcpy(host.data(), pass.ops.data(), ops_bytes);
+	if(!pass.chain.empty()) std::memcpy(host.data() + ch_off, pass.chain.data(), pass.chain.size() * sizeof(ChainEntry));
+	if(!phases.empty()) std::memcpy(host.data() + ph_off, phases.data(), phases.size() * sizeof(double2));
+	std::memcpy(host.data() + lb_off, lbits.data(), lbits.size() * sizeof(uint64_t));
+	upload_async(c, dev_prog, host.data(), need, "fused program upload");
+	unsigned char *dp = static_cast<unsigned char *>(dev_prog);
+	auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };  // the kernel's region layout
+	const size_t smem = (sizeof(typename Vec2<R>::type) << kStK) + a16(sizeof(uint64_t) << (kStK - g.m)) +
+	                    a16(lbits.size() * sizeof(uint64_t)) + phases.size() * sizeof(double2) + g.nops * sizeof(uint64_t) +
+	                    phases.size();
+	auto kern = g.narrow ? k_fused_stages<R, true> : k_fused_stages<R, false>;
+	check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "stage smem");
+	int per_sm = 1;
+	check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStThreads, smem), "stage occupancy");
+	const uint64_t grid = std::min<uint64_t>(g.ntiles - g.o_begin, (uint64_t)c.num_sms * std::max(1, per_sm));
+	kern<<<(unsigned)grid, kStThreads, smem, c.stream>>>(
+		static_cast<typename Vec2<R>::type *>(a), g, reinterpret_cast<const FusedOp *>(dp),
+		reinterpret_cast<const ChainEntry *>(dp + ch_off), reinterpret_cast<const double2 *>(dp + ph_off),
+		reinterpret_cast<const uint64_t *>(dp + lb_off));
+	after_launch(c, "fused stage pass");
+	return true;
+}
+
 }  // namespace
 
 void launch_fused_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, void *&dev_prog,
                        size_t &dev_prog_bytes) {
-	if(prec == TMFQS_FP64) run_fused<double>(c, a, pass, dev_prog, dev_prog_bytes);
-	else run_fused<float>(c, a, pass, dev_prog, dev_prog_bytes);
+	if(prec == TMFQS_FP64) {
+		if(!run_fused_stages<double>(c, a, pass, dev_prog, dev_prog_bytes)) run_fused<double>(c, a, pass, dev_prog, dev_prog_bytes);
+	} else {
+		run_fused<float>(c, a, pass, dev_prog, dev_prog_bytes);
+	}
 }
 
 void launch_bit_permutation(const LaunchCtx &c, int prec, void *a, unsigned n,
