@@ -987,6 +987,7 @@ struct StageGeom {
 	uint16_t tlo[kStMaxStages][16], thi[kStMaxStages][16];  // thread index nibbles -> local offset
 	uint8_t op_reg[kStMaxOps];                 // register bit of the op's Hadamard
 	uint16_t op_tab[kStMaxOps], op_lc[kStMaxOps];  // its chain: entries [tab, tab + lc) of the pass
+	uint8_t op_split[kStMaxOps];               // entries from here on have no register-bit control
 	uint8_t swz[3];                            // slot bit i ^= index bit swz[i] (0: none)
 };
 
@@ -1064,10 +1065,29 @@ __device__ __forceinline__ void stage_walk(uint32_t tw, const uint64_t (&rm)[kSt
 	}
 }
 
+// Walks one 32-entry word of entries that no register bit controls: each
+// applies to all 8 outputs of the thread or to none (tw), so the products of
+// the 8 outputs run unconditionally side by side.
+template <typename R, unsigned I, bool ALLNZ>
+__device__ __forceinline__ void stage_walk_uniform(uint32_t tw, uint32_t w, const double2 *cph, const bool (&nz)[8],
+                                                   typename Vec2<R>::type (&v)[16]) {
+	while(w) {
+		const unsigned e = __clz(w);
+		const uint32_t bit = 0x80000000u >> e;
+		w ^= bit;
+		if(tw & bit) {
+			const double2 c = cph[e];
+			const R pr = (R)c.x, pi = (R)c.y;
+#pragma unroll
+			for(unsigned p = 0; p < 8; ++p) st_cmul<R, ALLNZ>(pr, pi, v[st_r1<I>(p)], nz[p]);
+		}
+	}
+}
+
 template <typename R, unsigned I, bool NARROW>
 __device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R inv, bool chain, unsigned st, unsigned k,
-                                             const StageGeom &g, const uint64_t *lb, const double2 *ph, uint64_t cu,
-                                             unsigned t) {
+                                             const StageGeom &g, const uint64_t *lb, const double2 *ph, const uint8_t *ebit,
+                                             uint64_t base, unsigned t) {
 	typedef typename Vec2<R>::type V;
 	bool nz[8];
 #pragma unroll
@@ -1076,6 +1096,18 @@ __device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R 
 		nz[p] = butterfly<R>(v[r0], v[r1], inv) && !is_zero<R>(v[r1]);
 	}
 	if(!chain) return;
+	// The entries whose control is an outer bit set in this tile (one lane per
+	// entry, the same in every warp; entry e = bit 63 - e).
+	uint64_t cu = 0;
+	{
+		const unsigned lane = t & 31u, tab = g.op_tab[k], lc = g.op_lc[k];
+		for(unsigned e0 = 0; e0 < lc; e0 += 32) {
+			const unsigned e = e0 + lane;
+			const unsigned b = e < lc ? ebit[tab + e] : 0xffu;
+			const unsigned on = __ballot_sync(0xffffffffu, b != 0xffu && ((base >> b) & 1ull));
+			cu |= (uint64_t)__brev(on) << (e0 == 0 ? 32 : 0);
+		}
+	}
 	const uint64_t *L = lb + (size_t)k * kStK;
 	// Entries whose control is fixed for this thread: outer bits of the tile, the thread's local bits.
 	uint64_t tm = cu;
@@ -1090,18 +1122,29 @@ __device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R 
 		un |= rm[j];
 	}
 	const double2 *cph = ph + g.op_tab[k];
-	// The union over the warp's lanes: every lane walks the same entries.
-	const uint32_t wh = __reduce_or_sync(0xffffffffu, (uint32_t)(un >> 32));
-	const uint32_t wl = NARROW ? 0u : __reduce_or_sync(0xffffffffu, (uint32_t)un);
+	// Entries [0, split) may have register-bit controls (in the QFT: the
+	// stage's own lower bits, which come first in a chain); the rest are
+	// uniform per thread.  The walks go over the union of the warp's lanes.
+	const unsigned split = g.op_split[k];
+	const uint64_t pre = split ? (~0ull << (64 - split)) : 0ull;
+	const uint64_t upre = un & pre, upost = tm & ~pre;
+	const uint32_t wh = __reduce_or_sync(0xffffffffu, (uint32_t)(upre >> 32));
+	const uint32_t wl = NARROW ? 0u : __reduce_or_sync(0xffffffffu, (uint32_t)upre);
+	const uint32_t uh = __reduce_or_sync(0xffffffffu, (uint32_t)(upost >> 32));
+	const uint32_t ul = NARROW ? 0u : __reduce_or_sync(0xffffffffu, (uint32_t)upost);
 	bool all = true;
 #pragma unroll
 	for(unsigned p = 0; p < 8; ++p) all = all && nz[p];
 	if(all) {
 		stage_walk<R, I, 0, true>((uint32_t)(tm >> 32), rm, wh, cph, nz, v);
 		if constexpr(!NARROW) stage_walk<R, I, 1, true>((uint32_t)tm, rm, wl, cph + 32, nz, v);
+		stage_walk_uniform<R, I, true>((uint32_t)(tm >> 32), uh, cph, nz, v);
+		if constexpr(!NARROW) stage_walk_uniform<R, I, true>((uint32_t)tm, ul, cph + 32, nz, v);
 	} else {
 		stage_walk<R, I, 0, false>((uint32_t)(tm >> 32), rm, wh, cph, nz, v);
 		if constexpr(!NARROW) stage_walk<R, I, 1, false>((uint32_t)tm, rm, wl, cph + 32, nz, v);
+		stage_walk_uniform<R, I, false>((uint32_t)(tm >> 32), uh, cph, nz, v);
+		if constexpr(!NARROW) stage_walk_uniform<R, I, false>((uint32_t)tm, ul, cph + 32, nz, v);
 	}
 }
 
@@ -1118,11 +1161,10 @@ __global__ void __launch_bounds__(kStThreads, 2) k_fused_stages(typename Vec2<R>
 	V *s = reinterpret_cast<V *>(smem_raw);
 	const size_t o_hi = sizeof(V) * T, o_lb = o_hi + a16(sizeof(uint64_t) * nhi);
 	const size_t o_ph = o_lb + a16(sizeof(uint64_t) * g.nops * kStK), o_cu = o_ph + sizeof(double2) * g.nentries;
-	const size_t o_eb = o_cu + sizeof(uint64_t) * g.nops;
+	const size_t o_eb = o_cu;
 	uint64_t *hitab = reinterpret_cast<uint64_t *>(smem_raw + o_hi);
 	uint64_t *lb = reinterpret_cast<uint64_t *>(smem_raw + o_lb);
 	double2 *ph = reinterpret_cast<double2 *>(smem_raw + o_ph);
-	uint64_t *cus = reinterpret_cast<uint64_t *>(smem_raw + o_cu);
 	uint8_t *ebit = smem_raw + o_eb;  // per entry: its outer control bit, or 0xff for a local control
 	const unsigned t = threadIdx.x, lane = t & 31u, warp = t >> 5;
 	for(unsigned h = t; h < nhi; h += blockDim.x) {
@@ -1145,54 +1187,81 @@ __global__ void __launch_bounds__(kStThreads, 2) k_fused_stages(typename Vec2<R>
 	for(uint64_t o = g.o_begin + blockIdx.x; o < g.ntiles; o += gridDim.x) {
 		uint64_t base = o;
 		for(unsigned i = 0; i < kStK; ++i) base = insert0(base, g.lpos[i]);
-		for(unsigned j = t; j < T; j += blockDim.x) s[st_slot(j, g.swz)] = a[base | scatter(j)];
-		// The chain entries whose control is an outer bit set in this tile: one
-		// warp per op, one lane per entry (entry e = bit 63 - e).
-		for(unsigned k = warp; k < g.nops; k += blockDim.x >> 5) {
-			uint64_t u = 0;
-			for(unsigned e0 = 0; e0 < g.op_lc[k]; e0 += 32) {
-				const unsigned e = e0 + lane;
-				const unsigned b = e < g.op_lc[k] ? ebit[g.op_tab[k] + e] : 0xffu;
-				const unsigned on = __ballot_sync(0xffffffffu, b != 0xffu && ((base >> b) & 1ull));
-				u |= (uint64_t)__brev(on) << (e0 == 0 ? 32 : 0);
-			}
-			if(lane == 0) cus[k] = u;
-		}
-		__syncthreads();
 		for(unsigned st = 0; st < g.nstages; ++st) {
-			const unsigned jb = st_slot((unsigned)g.tlo[st][t & 15u] | g.thi[st][t >> 4], g.swz);
-			unsigned ro[kStRB];
-#pragma unroll
-			for(unsigned i = 0; i < kStRB; ++i) ro[i] = st_slot(1u << g.rbit[st][i], g.swz);
-			unsigned off[16];
-#pragma unroll
-			for(unsigned r = 0; r < 16; ++r) {
-				unsigned x = jb;
-#pragma unroll
-				for(unsigned i = 0; i < kStRB; ++i)
-					if((r >> i) & 1u) x ^= ro[i];
-				off[r] = x;
-			}
+			const bool first = st == 0, last = st + 1 == g.nstages;
+			const unsigned jl = (unsigned)g.tlo[st][t & 15u] | g.thi[st][t >> 4];  // the thread's local base index
 			V v[16];
+			if(first) {
+				// The first stage reads its amplitudes straight from HBM: global
+				// offsets are bit-linear in the local index (disjoint bits OR).
+				const uint64_t gb = base | scatter(jl);
+				uint64_t go[kStRB];
 #pragma unroll
-			for(unsigned r = 0; r < 16; ++r) v[r] = s[off[r]];
+				for(unsigned i = 0; i < kStRB; ++i) go[i] = scatter(1u << g.rbit[st][i]);
+#pragma unroll
+				for(unsigned r = 0; r < 16; ++r) {
+					uint64_t x = gb;
+#pragma unroll
+					for(unsigned i = 0; i < kStRB; ++i)
+						if((r >> i) & 1u) x |= go[i];
+					v[r] = a[x];
+				}
+			} else {
+				const unsigned jb = st_slot(jl, g.swz);
+				unsigned ro[kStRB];
+#pragma unroll
+				for(unsigned i = 0; i < kStRB; ++i) ro[i] = st_slot(1u << g.rbit[st][i], g.swz);
+#pragma unroll
+				for(unsigned r = 0; r < 16; ++r) {
+					unsigned x = jb;
+#pragma unroll
+					for(unsigned i = 0; i < kStRB; ++i)
+						if((r >> i) & 1u) x ^= ro[i];
+					v[r] = s[x];
+				}
+			}
 			const unsigned k1 = g.st_first[st] + g.st_count[st];
 			for(unsigned k = g.st_first[st]; k < k1; ++k) {
 				const bool chain_op = ops[k].kind == kFHChain;
-				const uint64_t cu = cus[k];
 				switch(g.op_reg[k]) {
-					case 0: stage_hchain<R, 0, NARROW>(v, inv, chain_op, st, k, g, lb, ph, cu, t); break;
-					case 1: stage_hchain<R, 1, NARROW>(v, inv, chain_op, st, k, g, lb, ph, cu, t); break;
-					case 2: stage_hchain<R, 2, NARROW>(v, inv, chain_op, st, k, g, lb, ph, cu, t); break;
-					default: stage_hchain<R, 3, NARROW>(v, inv, chain_op, st, k, g, lb, ph, cu, t); break;
+					case 0: stage_hchain<R, 0, NARROW>(v, inv, chain_op, st, k, g, lb, ph, ebit, base, t); break;
+					case 1: stage_hchain<R, 1, NARROW>(v, inv, chain_op, st, k, g, lb, ph, ebit, base, t); break;
+					case 2: stage_hchain<R, 2, NARROW>(v, inv, chain_op, st, k, g, lb, ph, ebit, base, t); break;
+					default: stage_hchain<R, 3, NARROW>(v, inv, chain_op, st, k, g, lb, ph, ebit, base, t); break;
 				}
 			}
+			if(last) {
+				// The last stage stores straight to HBM.
+				const uint64_t gb = base | scatter(jl);
+				uint64_t go[kStRB];
 #pragma unroll
-			for(unsigned r = 0; r < 16; ++r) s[off[r]] = v[r];
-			__syncthreads();
+				for(unsigned i = 0; i < kStRB; ++i) go[i] = scatter(1u << g.rbit[st][i]);
+#pragma unroll
+				for(unsigned r = 0; r < 16; ++r) {
+					uint64_t x = gb;
+#pragma unroll
+					for(unsigned i = 0; i < kStRB; ++i)
+						if((r >> i) & 1u) x |= go[i];
+					a[x] = v[r];
+				}
+			} else {
+				const unsigned jb = st_slot(jl, g.swz);
+				unsigned ro[kStRB];
+#pragma unroll
+				for(unsigned i = 0; i < kStRB; ++i) ro[i] = st_slot(1u << g.rbit[st][i], g.swz);
+#pragma unroll
+				for(unsigned r = 0; r < 16; ++r) {
+					unsigned x = jb;
+#pragma unroll
+					for(unsigned i = 0; i < kStRB; ++i)
+						if((r >> i) & 1u) x ^= ro[i];
+					s[x] = v[r];
+				}
+			}
+			// Between stages, and before the next tile's first stage writes the
+			// buffer the last one read.
+			if(!last || g.nstages > 1) __syncthreads();
 		}
-		for(unsigned j = t; j < T; j += blockDim.x) a[base | scatter(j)] = s[st_slot(j, g.swz)];
-		__syncthreads();
 	}
 }
 
@@ -1311,11 +1380,20 @@ bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phas
 		const unsigned lc = op.kind == kFHChain ? op.lc : 0u;
 		g.op_tab[k] = (uint16_t)phases.size();
 		g.op_lc[k] = (uint16_t)lc;
+		// The op's stage registers: entries after the last one they control are uniform per thread.
+		unsigned st = 0;
+		while(st + 1 < g.nstages && g.st_first[st + 1] <= k) ++st;
+		unsigned split = 0;
 		for(unsigned e = 0; e < lc; ++e) {
 			const ChainEntry &ce = pass.chain[op.tab + e];
 			phases.push_back(double2{ce.cr, ce.ci});
-			if(ce.local >= 0) lbits[(size_t)k * kStK + ce.local] |= 1ull << (63 - e);
+			if(ce.local >= 0) {
+				lbits[(size_t)k * kStK + ce.local] |= 1ull << (63 - e);
+				for(unsigned i = 0; i < kStRB; ++i)
+					if(g.rbit[st][i] == (unsigned)ce.local) split = e + 1;
+			}
 		}
+		g.op_split[k] = (uint8_t)split;
 	}
 	g.nentries = (unsigned)phases.size();
 	stage_swizzle(g);
@@ -1363,8 +1441,7 @@ bool run_fused_stages(const LaunchCtx &c, void *a, const FusedPass &pass, void *
 	unsigned char *dp = static_cast<unsigned char *>(dev_prog);
 	auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };  // the kernel's region layout
 	const size_t smem = (sizeof(typename Vec2<R>::type) << kStK) + a16(sizeof(uint64_t) << (kStK - g.m)) +
-	                    a16(lbits.size() * sizeof(uint64_t)) + phases.size() * sizeof(double2) + g.nops * sizeof(uint64_t) +
-	                    phases.size();
+	                    a16(lbits.size() * sizeof(uint64_t)) + phases.size() * sizeof(double2) + phases.size();
 	auto kern = g.narrow ? k_fused_stages<R, true> : k_fused_stages<R, false>;
 	check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "stage smem");
 	int per_sm = 1;
