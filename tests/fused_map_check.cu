@@ -127,6 +127,108 @@ static void check_pass(const char *name, const FusedPass &p) {
 	}
 }
 
+// The register-stage plan of a pass (plan_stages): each stage's register and
+// thread bits partition the tile, the op targets are register bits, the
+// shared slots are a bijection with conflict-free quarter-warps, every
+// thread's walk applies exactly the entries whose local control is set in
+// each of its |1> outputs, and no register-bit control follows op_split.
+// Prints per op the products its warps issue for local controls against
+// those its lanes need.
+static void check_stages(const char *name, const FusedPass &p) {
+	StageGeom g;
+	std::vector<double2> phases;
+	std::vector<uint64_t> tab;
+	const bool planned = plan_stages(p, g, phases, tab);
+	EXPECT(planned, "%s: no stage plan", name);
+	if(!planned) return;
+	const unsigned T = 1u << kStK;
+	std::vector<int> slot_seen(T, 0);
+	for(unsigned j = 0; j < T; ++j) ++slot_seen[stage_slot(j, g.scol)];
+	for(unsigned j = 0; j < T; ++j) EXPECT(slot_seen[j] == 1, "%s: slot %u used %d times", name, j, slot_seen[j]);
+	for(unsigned st = 0; st < g.nstages; ++st) {
+		unsigned all = 0;
+		for(unsigned i = 0; i < kStRB; ++i) all |= 1u << g.rbit[st][i];
+		for(unsigned i = 0; i < kStTB; ++i) all |= 1u << g.tbit[st][i];
+		EXPECT(all == T - 1, "%s stage %u: bits do not partition the tile", name, st);
+		std::vector<int> seen(T, 0);
+		for(unsigned t = 0; t < kStThreads; ++t) {
+			const unsigned jl = (unsigned)g.geo[st][kStGeoTlo + (t & 15u)] | g.geo[st][kStGeoThi + (t >> 4)];
+			unsigned want = 0;
+			for(unsigned i = 0; i < kStTB; ++i)
+				if((t >> i) & 1u) want |= 1u << g.tbit[st][i];
+			EXPECT(jl == want, "%s stage %u: local base of thread %u", name, st, t);
+			const unsigned jb = (unsigned)g.geo[st][kStGeoSlo + (t & 15u)] ^ g.geo[st][kStGeoShi + (t >> 4)];
+			for(unsigned r = 0; r < 16; ++r) {
+				unsigned j = jl, x = jb;
+				for(unsigned i = 0; i < kStRB; ++i)
+					if((r >> i) & 1u) {
+						j |= 1u << g.rbit[st][i];
+						x ^= g.geo[st][kStGeoReg + i];
+					}
+				++seen[j];
+				EXPECT(x == stage_slot(j, g.scol), "%s stage %u: slot of thread %u register %u", name, st, t, r);
+			}
+		}
+		for(unsigned j = 0; j < T; ++j) EXPECT(seen[j] == 1, "%s stage %u: amplitude %u covered %d times", name, st, j, seen[j]);
+		for(unsigned t0 = 0; t0 < kStThreads; t0 += 8)
+			for(unsigned r = 0; r < 16; ++r) {
+				std::set<unsigned> groups;
+				for(unsigned t = t0; t < t0 + 8; ++t) {
+					unsigned x = (unsigned)g.geo[st][kStGeoSlo + (t & 15u)] ^ g.geo[st][kStGeoShi + (t >> 4)];
+					for(unsigned i = 0; i < kStRB; ++i)
+						if((r >> i) & 1u) x ^= g.geo[st][kStGeoReg + i];
+					groups.insert(x & 7u);
+				}
+				EXPECT(groups.size() == 8, "%s stage %u: quarter-warp at thread %u register %u has %zu bank groups", name, st,
+				       t0, r, groups.size());
+			}
+		for(unsigned k = g.st_first[st]; k < g.st_first[st] + g.st_count[st]; ++k) {
+			const FusedOp &op = p.ops[k];
+			EXPECT(g.rbit[st][g.op_reg[k]] == op.lt, "%s op %u: target is not its register bit", name, k);
+			const uint64_t *Tb = tab.data() + (size_t)k * kStTabWords;
+			const unsigned I = g.op_reg[k];
+			uint64_t rall = 0;
+			for(unsigned i = 0; i < kStRB; ++i) rall |= Tb[kStTabReg + i];
+			EXPECT(rall == Tb[kStTabRegAll], "%s op %u: register union", name, k);
+			EXPECT(Tb[kStTabReg + I] == 0, "%s op %u: entry controlled by its own target", name, k);
+			const unsigned split = g.op_split[k];
+			const uint64_t post = split ? ~(~0ull << (64 - split)) : ~0ull;
+			EXPECT((rall & post) == 0, "%s op %u: register control after the split", name, k);
+			double issued = 0.0, needed = 0.0;
+			for(unsigned w = 0; w < kStThreads / 32; ++w) {
+				uint64_t wu = 0;
+				for(unsigned l = 0; l < 32; ++l) {
+					const unsigned t = 32 * w + l;
+					const uint64_t tm = Tb[kStTabLo + (t & 15u)] | Tb[kStTabHi + (t >> 4)];
+					wu |= tm;
+					const unsigned jl = (unsigned)g.geo[st][kStGeoTlo + (t & 15u)] | g.geo[st][kStGeoThi + (t >> 4)];
+					for(unsigned r = 0; r < 16; ++r) {
+						if(!((r >> I) & 1u)) continue;  // |1> outputs only
+						unsigned j1 = jl;
+						uint64_t got = tm;
+						for(unsigned i = 0; i < kStRB; ++i)
+							if((r >> i) & 1u) {
+								j1 |= 1u << g.rbit[st][i];
+								got |= Tb[kStTabReg + i];
+							}
+						uint64_t want = 0;
+						for(unsigned e = 0; e < op.lc; ++e) {
+							const ChainEntry &ce = p.chain[op.tab + e];
+							if(ce.local >= 0 && ((j1 >> ce.local) & 1u)) want |= 1ull << (63 - e);
+						}
+						EXPECT(got == want, "%s op %u: mask of thread %u register %u", name, k, t, r);
+						needed += (double)__builtin_popcountll(want & ~rall);
+					}
+				}
+				EXPECT(wu == Tb[kStTabWarp + w], "%s op %u: warp %u union", name, k, w);
+				issued += 32.0 * 8.0 * (double)__builtin_popcountll(wu & ~rall);
+			}
+			std::printf("stage %s op %u stage %u lt %u pairs %u issued %.0f needed %.0f\n", name, k, st, op.lt, T / 2, issued,
+			            needed);
+		}
+	}
+}
+
 int main() {
 	// QFT-28 in the exact complex128 form: tiles of 12 local bits, bits 0..2
 	// always local; passes of 9 Hadamard bits, then the 10 lowest.
@@ -150,6 +252,11 @@ int main() {
 	check_pass("qft28_p2", pass_of(28, 18, 10));
 	check_pass("qft28_p3", pass_of(28, 9, 0));
 	check_pass("qft32_p1", pass_of(32, 31, 23));
+	check_stages("qft28_p1", pass_of(28, 27, 19));
+	check_stages("qft28_p2", pass_of(28, 18, 10));
+	check_stages("qft28_p3", pass_of(28, 9, 0));
+	check_stages("qft32_p1", pass_of(32, 31, 23));
+	check_stages("qft32_p4", pass_of(32, 4, 0));
 	// Scattered controls: every other lower bit, and a repeated control.
 	check_pass("scattered", make(24, {0, 1, 2, 5, 7, 9, 11, 13, 15, 17, 19, 21}, {21, 17, 13, 9},
 	                             [](unsigned b) {
@@ -159,6 +266,14 @@ int main() {
 		                             c.push_back(1);
 		                             return c;
 	                             }));
+	check_stages("scattered", make(24, {0, 1, 2, 5, 7, 9, 11, 13, 15, 17, 19, 21}, {21, 17, 13, 9},
+	                               [](unsigned b) {
+		                               std::vector<unsigned> c;
+		                               for(int x = (int)b - 2; x >= 0; x -= 2) c.push_back((unsigned)x);
+		                               c.push_back(1);
+		                               c.push_back(1);
+		                               return c;
+	                               }));
 	// Seven local bits (the smallest mapped tile) and 13 (complex64).
 	check_pass("k7", make(7, {0, 1, 2, 3, 4, 5, 6}, {6, 5, 4, 3}, below));
 	check_pass("k13", make(30, {0, 1, 2, 3, 20, 21, 22, 23, 24, 25, 26, 27, 28}, {28, 27, 26, 25, 24, 23, 22, 21, 20}, below));

@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <vector>
 
 #include "device_common.cuh"
@@ -959,21 +960,35 @@ void run_perm(const LaunchCtx &c, void *a, unsigned n, const std::vector<std::pa
 // of its chain's controlled phases as separately rounded complex products on
 // the |1> outputs whose control bit is set -- the same IEEE operations, in the
 // same order per amplitude, as the per-gate path (dense_state_backend.cpp:
-// 255-304), so the result is bit-identical.  A stage reads and writes the tile
-// in shared memory once and takes one barrier (instead of one of each per
-// op), and each Hadamard's 8 |1> outputs are 8 independent chains of dependent
-// products per thread.  The controls of a chain entry are an outer bit (set or
-// not for the whole tile), a local bit that indexes the thread (set or not
-// for the thread), or a register bit (set for half of the thread's outputs).
-// Lanes walk the entries of the warp's union mask together (one broadcast
-// phase load per entry); each output applies those in its own mask.
+// 255-304), so the result is bit-identical.  The first stage reads the tile
+// from HBM, the last writes it back, the ones between pass it on through
+// shared memory with one barrier each.  Each Hadamard's 8 |1> outputs are 8
+// independent chains of dependent products per thread.
+//
+// The control of a chain entry is an outer bit (set or not for the whole
+// tile), a local bit that indexes the thread (set or not per thread), or a
+// register bit (set for half of a thread's outputs).  Lanes walk the entries
+// of their warp's union together (one broadcast phase load per entry), so an
+// entry whose control is a lane bit costs every lane its products while half
+// of them need none.  The host therefore picks per stage which local bits are
+// register, lane and warp bits: fillers of the register bits are the most
+// frequent controls, lanes the least frequent (no control at all wherever the
+// tile has such bits).  The thread masks of every op come from host tables.
 // ---------------------------------------------------------------------------
-constexpr unsigned kStRB = 4;               // register bits per stage
-constexpr unsigned kStK = 12;               // local bits of a tile (complex128: 64 KiB)
-constexpr unsigned kStThreads = 1u << (kStK - kStRB);
+constexpr unsigned kStRB = 4;                    // register bits per stage
+constexpr unsigned kStK = 12;                    // local bits of a tile (complex128: 64 KiB)
+constexpr unsigned kStTB = kStK - kStRB;         // thread index bits (0-4: the lane, 5-7: the warp)
+constexpr unsigned kStThreads = 1u << kStTB;
 constexpr unsigned kStMaxOps = 16;
 constexpr unsigned kStMaxStages = 8;
 constexpr unsigned kStMaxEntries = 1024;
+// Per-op table of 64-bit entry masks (entry e = bit 63 - e): the entries
+// controlled by the thread index's low and high nibble, the union over each
+// warp's lanes, the entries controlled by each register bit, their union.
+constexpr unsigned kStTabLo = 0, kStTabHi = 16, kStTabWarp = 32, kStTabReg = 40, kStTabRegAll = 44, kStTabWords = 48;
+// Per-stage table of 16-bit offsets: thread nibbles -> local index (lo, hi)
+// and -> shared slot (lo, hi), register bits -> shared slot.
+constexpr unsigned kStGeoTlo = 0, kStGeoThi = 16, kStGeoSlo = 32, kStGeoShi = 48, kStGeoReg = 64, kStGeoWords = 68;
 
 struct StageGeom {
 	unsigned n, m;
@@ -982,25 +997,14 @@ struct StageGeom {
 	unsigned nops, nstages, nentries, narrow;
 	double inv;
 	uint8_t st_first[kStMaxStages], st_count[kStMaxStages];
-	uint8_t rbit[kStMaxStages][kStRB];        // local bit of register bit i
-	uint8_t tbit[kStMaxStages][kStK - kStRB];  // local bit of thread index bit k
-	uint16_t tlo[kStMaxStages][16], thi[kStMaxStages][16];  // thread index nibbles -> local offset
-	uint8_t op_reg[kStMaxOps];                 // register bit of the op's Hadamard
+	uint8_t rbit[kStMaxStages][kStRB];  // local bit of register bit i
+	uint8_t tbit[kStMaxStages][kStTB];  // local bit of thread index bit k
+	uint16_t geo[kStMaxStages][kStGeoWords];
+	uint8_t op_reg[kStMaxOps];                     // register bit of the op's Hadamard
 	uint16_t op_tab[kStMaxOps], op_lc[kStMaxOps];  // its chain: entries [tab, tab + lc) of the pass
-	uint8_t op_split[kStMaxOps];               // entries from here on have no register-bit control
-	uint8_t swz[3];                            // slot bit i ^= index bit swz[i] (0: none)
+	uint8_t op_split[kStMaxOps];                   // entries from here on have no register-bit control
+	uint8_t scol[kStK];                            // shared slot of j: j ^ XOR of scol[b] over bits b >= 3 of j
 };
-
-// Shared slot of local index j: bits 0-2 XORed with three higher bits chosen
-// per pass (stage_swizzle) so that each stage's quarter-warps read 8 distinct
-// 16-byte bank groups.  XOR-linear: slot(a ^ b) = slot(a) ^ slot(b).
-__device__ __forceinline__ unsigned st_slot(unsigned j, const uint8_t (&swz)[3]) {
-	unsigned x = j;
-#pragma unroll
-	for(unsigned i = 0; i < 3; ++i)
-		if(swz[i]) x ^= ((j >> swz[i]) & 1u) << i;
-	return x;
-}
 
 // The |1> output p (of the 8 of a Hadamard on register bit I) is register r1(p).
 template <unsigned I>
@@ -1008,10 +1012,32 @@ __device__ __forceinline__ constexpr unsigned st_r1(unsigned p) {
 	return ((p >> I) << (I + 1)) | (p & ((1u << I) - 1u)) | (1u << I);
 }
 
+// Zero tests on the bit patterns (+0 and -0 compare equal to zero; so does
+// this), on the integer units instead of the FP64 pipe.
+__device__ __forceinline__ unsigned st_bits_nonsign(double2 x) {
+	return ((unsigned)(__double2hiint(x.x) | __double2hiint(x.y)) << 1) | (unsigned)__double2loint(x.x) |
+	       (unsigned)__double2loint(x.y);
+}
+__device__ __forceinline__ unsigned st_bits_nonsign(float2 x) {
+	return (__float_as_uint(x.x) | __float_as_uint(x.y)) << 1;
+}
+
+// Hadamard butterfly (dense_state_backend.cpp:265-271) without the zero test.
+template <typename R>
+__device__ __forceinline__ void st_bfly(typename Vec2<R>::type &x, typename Vec2<R>::type &y, R inv) {
+	typename Vec2<R>::type o0, o1;
+	o0.x = rmul(radd(x.x, y.x), inv);
+	o0.y = rmul(radd(x.y, y.y), inv);
+	o1.x = rmul(rsub(x.x, y.x), inv);
+	o1.y = rmul(rsub(x.y, y.y), inv);
+	x = o0;
+	y = o1;
+}
+
 // One rounded complex product (dense_state_backend.cpp:300-301) on output p
 // when `on`: computed unconditionally and kept by a select, so that the
 // products of independent outputs interleave (a skipped product leaves the
-// value exactly as it was).  ALLNZ: every output is nonzero (the common case).
+// value exactly as it was).  ALLNZ: every output of the warp is nonzero.
 template <typename R, bool ALLNZ>
 __device__ __forceinline__ void st_cmul(R pr, R pi, typename Vec2<R>::type &x, bool on) {
 	R re = x.x, im = x.y;
@@ -1034,147 +1060,188 @@ __device__ __forceinline__ void st_apply_reg(R pr, R pi, const bool (&nz)[8], ty
 		if((st_r1<I>(p) >> J) & 1u) st_cmul<R, ALLNZ>(pr, pi, v[st_r1<I>(p)], nz[p]);
 }
 
-// Walks one 32-entry word W (H: high word of the masks, else low) of the
-// warp's union of entries in circuit order.  An entry controlled by a
-// register bit goes to the outputs with that bit set; any other entry (an
-// outer bit or a thread bit: the same for all of this thread's outputs) to all
-// 8 when the thread's mask tw has it.  Zero outputs are skipped (nz).
+// Walks one 32-entry word W (0: high word of the masks) of the warp's union
+// of entries in circuit order.  An entry controlled by a register bit (ra)
+// goes to the outputs with that bit set; any other entry (an outer bit or a
+// thread bit: the same for all of this thread's outputs) to all 8 when the
+// thread's mask tw has it.  The next entry's phase is loaded while this one's
+// products run.
 template <typename R, unsigned I, int W, bool ALLNZ>
-__device__ __forceinline__ void stage_walk(uint32_t tw, const uint64_t (&rm)[kStRB], uint32_t w, const double2 *cph,
-                                           const bool (&nz)[8], typename Vec2<R>::type (&v)[16]) {
+__device__ __forceinline__ void stage_walk(uint32_t tw, const uint64_t (&rm)[kStRB], uint64_t rall, uint32_t w,
+                                           const double2 *cph, const bool (&nz)[8], typename Vec2<R>::type (&v)[16]) {
+	if(!w) return;
+	const uint32_t ra = W ? (uint32_t)rall : (uint32_t)(rall >> 32);
 	const uint32_t r0 = W ? (uint32_t)rm[0] : (uint32_t)(rm[0] >> 32), r1 = W ? (uint32_t)rm[1] : (uint32_t)(rm[1] >> 32);
-	const uint32_t r2 = W ? (uint32_t)rm[2] : (uint32_t)(rm[2] >> 32), r3 = W ? (uint32_t)rm[3] : (uint32_t)(rm[3] >> 32);
-	while(w) {
-		const unsigned e = __clz(w);
+	const uint32_t r2 = W ? (uint32_t)rm[2] : (uint32_t)(rm[2] >> 32);
+	unsigned e = __clz(w);
+	double2 c = cph[e];
+	for(;;) {
 		const uint32_t bit = 0x80000000u >> e;
 		w ^= bit;
-		const double2 c = cph[e];
 		const R pr = (R)c.x, pi = (R)c.y;
-		if(r0 & bit) {
-			if constexpr(I != 0) st_apply_reg<R, I, 0, ALLNZ>(pr, pi, nz, v);
-		} else if(r1 & bit) {
-			if constexpr(I != 1) st_apply_reg<R, I, 1, ALLNZ>(pr, pi, nz, v);
-		} else if(r2 & bit) {
-			if constexpr(I != 2) st_apply_reg<R, I, 2, ALLNZ>(pr, pi, nz, v);
-		} else if(r3 & bit) {
-			if constexpr(I != 3) st_apply_reg<R, I, 3, ALLNZ>(pr, pi, nz, v);
+		if(w) {
+			e = __clz(w);
+			c = cph[e];
+		}
+		if(ra & bit) {
+			if(r0 & bit) {
+				if constexpr(I != 0) st_apply_reg<R, I, 0, ALLNZ>(pr, pi, nz, v);
+			} else if(r1 & bit) {
+				if constexpr(I != 1) st_apply_reg<R, I, 1, ALLNZ>(pr, pi, nz, v);
+			} else if(r2 & bit) {
+				if constexpr(I != 2) st_apply_reg<R, I, 2, ALLNZ>(pr, pi, nz, v);
+			} else {
+				if constexpr(I != 3) st_apply_reg<R, I, 3, ALLNZ>(pr, pi, nz, v);
+			}
 		} else if(tw & bit) {
 #pragma unroll
 			for(unsigned p = 0; p < 8; ++p) st_cmul<R, ALLNZ>(pr, pi, v[st_r1<I>(p)], nz[p]);
 		}
+		if(!w) break;
 	}
 }
 
 // Walks one 32-entry word of entries that no register bit controls: each
-// applies to all 8 outputs of the thread or to none (tw), so the products of
-// the 8 outputs run unconditionally side by side.
+// applies to all 8 outputs of the thread or to none (tw).
 template <typename R, unsigned I, bool ALLNZ>
 __device__ __forceinline__ void stage_walk_uniform(uint32_t tw, uint32_t w, const double2 *cph, const bool (&nz)[8],
                                                    typename Vec2<R>::type (&v)[16]) {
-	while(w) {
-		const unsigned e = __clz(w);
+	if(!w) return;
+	unsigned e = __clz(w);
+	double2 c = cph[e];
+	for(;;) {
 		const uint32_t bit = 0x80000000u >> e;
 		w ^= bit;
+		const R pr = (R)c.x, pi = (R)c.y;
+		if(w) {
+			e = __clz(w);
+			c = cph[e];
+		}
 		if(tw & bit) {
-			const double2 c = cph[e];
-			const R pr = (R)c.x, pi = (R)c.y;
 #pragma unroll
 			for(unsigned p = 0; p < 8; ++p) st_cmul<R, ALLNZ>(pr, pi, v[st_r1<I>(p)], nz[p]);
 		}
+		if(!w) break;
 	}
 }
 
+// One op of a stage: the Hadamard on register bit I (all-zero pairs are left
+// as they are), then, for an H-chain, its controlled phases.
 template <typename R, unsigned I, bool NARROW>
-__device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R inv, bool chain, unsigned st, unsigned k,
-                                             const StageGeom &g, const uint64_t *lb, const double2 *ph, const uint8_t *ebit,
-                                             uint64_t base, unsigned t) {
-	typedef typename Vec2<R>::type V;
-	bool nz[8];
+__device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R inv, bool chain, unsigned k,
+                                             const StageGeom &g, const uint64_t *tab, const double2 *ph,
+                                             const uint8_t *ebit, uint64_t base, unsigned t) {
+	unsigned pz = 0;  // some pair of this thread is all zero
 #pragma unroll
 	for(unsigned p = 0; p < 8; ++p) {
-		const unsigned r0 = ((p >> I) << (I + 1)) | (p & ((1u << I) - 1u)), r1 = r0 | (1u << I);
-		nz[p] = butterfly<R>(v[r0], v[r1], inv) && !is_zero<R>(v[r1]);
+		const unsigned r1 = st_r1<I>(p), r0 = r1 ^ (1u << I);
+		pz |= (st_bits_nonsign(v[r0]) | st_bits_nonsign(v[r1])) == 0u;
+	}
+	if(__any_sync(0xffffffffu, pz)) {
+#pragma unroll
+		for(unsigned p = 0; p < 8; ++p) {
+			const unsigned r1 = st_r1<I>(p), r0 = r1 ^ (1u << I);
+			if((st_bits_nonsign(v[r0]) | st_bits_nonsign(v[r1])) != 0u) st_bfly<R>(v[r0], v[r1], inv);
+		}
+	} else {
+#pragma unroll
+		for(unsigned p = 0; p < 8; ++p) {
+			const unsigned r1 = st_r1<I>(p), r0 = r1 ^ (1u << I);
+			st_bfly<R>(v[r0], v[r1], inv);
+		}
 	}
 	if(!chain) return;
+	bool nz[8];
+	bool mine = true;
+#pragma unroll
+	for(unsigned p = 0; p < 8; ++p) {
+		nz[p] = st_bits_nonsign(v[st_r1<I>(p)]) != 0u;
+		mine = mine && nz[p];
+	}
+	const bool all = __all_sync(0xffffffffu, mine);
 	// The entries whose control is an outer bit set in this tile (one lane per
-	// entry, the same in every warp; entry e = bit 63 - e).
+	// entry, the same in every warp).
 	uint64_t cu = 0;
 	{
-		const unsigned lane = t & 31u, tab = g.op_tab[k], lc = g.op_lc[k];
+		const unsigned lane = t & 31u, tb = g.op_tab[k], lc = g.op_lc[k];
 		for(unsigned e0 = 0; e0 < lc; e0 += 32) {
 			const unsigned e = e0 + lane;
-			const unsigned b = e < lc ? ebit[tab + e] : 0xffu;
+			const unsigned b = e < lc ? ebit[tb + e] : 0xffu;
 			const unsigned on = __ballot_sync(0xffffffffu, b != 0xffu && ((base >> b) & 1ull));
 			cu |= (uint64_t)__brev(on) << (e0 == 0 ? 32 : 0);
 		}
 	}
-	const uint64_t *L = lb + (size_t)k * kStK;
-	// Entries whose control is fixed for this thread: outer bits of the tile, the thread's local bits.
-	uint64_t tm = cu;
-#pragma unroll
-	for(unsigned b = 0; b < kStK - kStRB; ++b)
-		if((t >> b) & 1u) tm |= L[g.tbit[st][b]];
+	const uint64_t *T = tab + (size_t)k * kStTabWords;
+	const uint64_t tm = cu | T[kStTabLo + (t & 15u)] | T[kStTabHi + (t >> 4)];  // this thread's fixed controls
+	const uint64_t wu = cu | T[kStTabWarp + (t >> 5)];                          // their union over the warp
+	const uint64_t rall = T[kStTabRegAll];
 	uint64_t rm[kStRB];
-	uint64_t un = tm;
 #pragma unroll
-	for(unsigned j = 0; j < kStRB; ++j) {
-		rm[j] = j == I ? 0ull : L[g.rbit[st][j]];
-		un |= rm[j];
-	}
+	for(unsigned j = 0; j < kStRB; ++j) rm[j] = T[kStTabReg + j];
 	const double2 *cph = ph + g.op_tab[k];
-	// Entries [0, split) may have register-bit controls (in the QFT: the
-	// stage's own lower bits, which come first in a chain); the rest are
-	// uniform per thread.  The walks go over the union of the warp's lanes.
+	// Entries [0, split) may have register-bit controls; the rest are uniform
+	// per thread.
 	const unsigned split = g.op_split[k];
 	const uint64_t pre = split ? (~0ull << (64 - split)) : 0ull;
-	const uint64_t upre = un & pre, upost = tm & ~pre;
-	const uint32_t wh = __reduce_or_sync(0xffffffffu, (uint32_t)(upre >> 32));
-	const uint32_t wl = NARROW ? 0u : __reduce_or_sync(0xffffffffu, (uint32_t)upre);
-	const uint32_t uh = __reduce_or_sync(0xffffffffu, (uint32_t)(upost >> 32));
-	const uint32_t ul = NARROW ? 0u : __reduce_or_sync(0xffffffffu, (uint32_t)upost);
-	bool all = true;
-#pragma unroll
-	for(unsigned p = 0; p < 8; ++p) all = all && nz[p];
+	const uint64_t upre = (wu | rall) & pre, upost = wu & ~pre;
+	const uint32_t wh = (uint32_t)(upre >> 32), wl = (uint32_t)upre;
+	const uint32_t uh = (uint32_t)(upost >> 32), ul = (uint32_t)upost;
 	if(all) {
-		stage_walk<R, I, 0, true>((uint32_t)(tm >> 32), rm, wh, cph, nz, v);
-		if constexpr(!NARROW) stage_walk<R, I, 1, true>((uint32_t)tm, rm, wl, cph + 32, nz, v);
+		stage_walk<R, I, 0, true>((uint32_t)(tm >> 32), rm, rall, wh, cph, nz, v);
+		if constexpr(!NARROW) stage_walk<R, I, 1, true>((uint32_t)tm, rm, rall, wl, cph + 32, nz, v);
 		stage_walk_uniform<R, I, true>((uint32_t)(tm >> 32), uh, cph, nz, v);
 		if constexpr(!NARROW) stage_walk_uniform<R, I, true>((uint32_t)tm, ul, cph + 32, nz, v);
 	} else {
-		stage_walk<R, I, 0, false>((uint32_t)(tm >> 32), rm, wh, cph, nz, v);
-		if constexpr(!NARROW) stage_walk<R, I, 1, false>((uint32_t)tm, rm, wl, cph + 32, nz, v);
+		stage_walk<R, I, 0, false>((uint32_t)(tm >> 32), rm, rall, wh, cph, nz, v);
+		if constexpr(!NARROW) stage_walk<R, I, 1, false>((uint32_t)tm, rm, rall, wl, cph + 32, nz, v);
 		stage_walk_uniform<R, I, false>((uint32_t)(tm >> 32), uh, cph, nz, v);
 		if constexpr(!NARROW) stage_walk_uniform<R, I, false>((uint32_t)tm, ul, cph + 32, nz, v);
 	}
 }
 
+// Shared-memory regions of k_fused_stages, at 16-byte boundaries (phases are
+// read as 16-byte values): tile, outer-offset table, op tables, phases, stage
+// tables, outer control bits.
+struct StageSmem {
+	size_t hi, tab, ph, geo, eb, total;
+};
+__host__ __device__ inline StageSmem stage_smem_layout(size_t amp_bytes, unsigned m, unsigned nops, unsigned nentries,
+                                                       unsigned nstages) {
+	auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+	StageSmem l;
+	l.hi = amp_bytes << kStK;
+	l.tab = l.hi + a16(sizeof(uint64_t) << (kStK - m));
+	l.ph = l.tab + a16(sizeof(uint64_t) * nops * kStTabWords);
+	l.geo = l.ph + sizeof(double2) * nentries;
+	l.eb = l.geo + a16(sizeof(uint16_t) * nstages * kStGeoWords);
+	l.total = l.eb + nentries;
+	return l;
+}
+
 template <typename R, bool NARROW>
 __global__ void __launch_bounds__(kStThreads, 2) k_fused_stages(typename Vec2<R>::type *a, const __grid_constant__ StageGeom g,
-                                                                const FusedOp *ops, const ChainEntry *chain,
-                                                                const double2 *gph, const uint64_t *glb) {
+                                                                const ChainEntry *chain, const double2 *gph,
+                                                                const uint64_t *gtab) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
-	constexpr unsigned T = 1u << kStK;
+	const StageSmem L = stage_smem_layout(sizeof(V), g.m, g.nops, g.nentries, g.nstages);
 	const unsigned nhi = 1u << (kStK - g.m);
-	// Regions at 16-byte boundaries (the phases are read as 16-byte values).
-	auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
 	V *s = reinterpret_cast<V *>(smem_raw);
-	const size_t o_hi = sizeof(V) * T, o_lb = o_hi + a16(sizeof(uint64_t) * nhi);
-	const size_t o_ph = o_lb + a16(sizeof(uint64_t) * g.nops * kStK), o_cu = o_ph + sizeof(double2) * g.nentries;
-	const size_t o_eb = o_cu;
-	uint64_t *hitab = reinterpret_cast<uint64_t *>(smem_raw + o_hi);
-	uint64_t *lb = reinterpret_cast<uint64_t *>(smem_raw + o_lb);
-	double2 *ph = reinterpret_cast<double2 *>(smem_raw + o_ph);
-	uint8_t *ebit = smem_raw + o_eb;  // per entry: its outer control bit, or 0xff for a local control
-	const unsigned t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+	uint64_t *hitab = reinterpret_cast<uint64_t *>(smem_raw + L.hi);
+	uint64_t *tab = reinterpret_cast<uint64_t *>(smem_raw + L.tab);
+	double2 *ph = reinterpret_cast<double2 *>(smem_raw + L.ph);
+	uint16_t *geo = reinterpret_cast<uint16_t *>(smem_raw + L.geo);
+	uint8_t *ebit = smem_raw + L.eb;  // per entry: its outer control bit, or 0xff for a local control
+	const unsigned t = threadIdx.x;
 	for(unsigned h = t; h < nhi; h += blockDim.x) {
 		uint64_t v = 0;
 		for(unsigned i = 0; i < kStK - g.m; ++i)
 			if((h >> i) & 1u) v |= 1ull << g.lpos[g.m + i];
 		hitab[h] = v;
 	}
-	for(unsigned e = t; e < g.nops * kStK; e += blockDim.x) lb[e] = glb[e];
+	for(unsigned e = t; e < g.nops * kStTabWords; e += blockDim.x) tab[e] = gtab[e];
 	for(unsigned e = t; e < g.nentries; e += blockDim.x) ph[e] = gph[e];
+	for(unsigned e = t; e < g.nstages * kStGeoWords; e += blockDim.x) geo[e] = g.geo[e / kStGeoWords][e % kStGeoWords];
 	for(unsigned k = 0; k < g.nops; ++k)
 		for(unsigned e = t; e < g.op_lc[k]; e += blockDim.x) {
 			const ChainEntry ce = chain[g.op_tab[k] + e];
@@ -1189,12 +1256,12 @@ __global__ void __launch_bounds__(kStThreads, 2) k_fused_stages(typename Vec2<R>
 		for(unsigned i = 0; i < kStK; ++i) base = insert0(base, g.lpos[i]);
 		for(unsigned st = 0; st < g.nstages; ++st) {
 			const bool first = st == 0, last = st + 1 == g.nstages;
-			const unsigned jl = (unsigned)g.tlo[st][t & 15u] | g.thi[st][t >> 4];  // the thread's local base index
+			const uint16_t *G = geo + st * kStGeoWords;
 			V v[16];
 			if(first) {
 				// The first stage reads its amplitudes straight from HBM: global
 				// offsets are bit-linear in the local index (disjoint bits OR).
-				const uint64_t gb = base | scatter(jl);
+				const uint64_t gb = base | scatter((unsigned)G[kStGeoTlo + (t & 15u)] | G[kStGeoThi + (t >> 4)]);
 				uint64_t go[kStRB];
 #pragma unroll
 				for(unsigned i = 0; i < kStRB; ++i) go[i] = scatter(1u << g.rbit[st][i]);
@@ -1207,10 +1274,10 @@ __global__ void __launch_bounds__(kStThreads, 2) k_fused_stages(typename Vec2<R>
 					v[r] = a[x];
 				}
 			} else {
-				const unsigned jb = st_slot(jl, g.swz);
+				const unsigned jb = (unsigned)G[kStGeoSlo + (t & 15u)] ^ G[kStGeoShi + (t >> 4)];
 				unsigned ro[kStRB];
 #pragma unroll
-				for(unsigned i = 0; i < kStRB; ++i) ro[i] = st_slot(1u << g.rbit[st][i], g.swz);
+				for(unsigned i = 0; i < kStRB; ++i) ro[i] = G[kStGeoReg + i];
 #pragma unroll
 				for(unsigned r = 0; r < 16; ++r) {
 					unsigned x = jb;
@@ -1222,17 +1289,17 @@ __global__ void __launch_bounds__(kStThreads, 2) k_fused_stages(typename Vec2<R>
 			}
 			const unsigned k1 = g.st_first[st] + g.st_count[st];
 			for(unsigned k = g.st_first[st]; k < k1; ++k) {
-				const bool chain_op = ops[k].kind == kFHChain;
+				const bool chain_op = g.op_lc[k] != 0;
 				switch(g.op_reg[k]) {
-					case 0: stage_hchain<R, 0, NARROW>(v, inv, chain_op, st, k, g, lb, ph, ebit, base, t); break;
-					case 1: stage_hchain<R, 1, NARROW>(v, inv, chain_op, st, k, g, lb, ph, ebit, base, t); break;
-					case 2: stage_hchain<R, 2, NARROW>(v, inv, chain_op, st, k, g, lb, ph, ebit, base, t); break;
-					default: stage_hchain<R, 3, NARROW>(v, inv, chain_op, st, k, g, lb, ph, ebit, base, t); break;
+					case 0: stage_hchain<R, 0, NARROW>(v, inv, chain_op, k, g, tab, ph, ebit, base, t); break;
+					case 1: stage_hchain<R, 1, NARROW>(v, inv, chain_op, k, g, tab, ph, ebit, base, t); break;
+					case 2: stage_hchain<R, 2, NARROW>(v, inv, chain_op, k, g, tab, ph, ebit, base, t); break;
+					default: stage_hchain<R, 3, NARROW>(v, inv, chain_op, k, g, tab, ph, ebit, base, t); break;
 				}
 			}
 			if(last) {
 				// The last stage stores straight to HBM.
-				const uint64_t gb = base | scatter(jl);
+				const uint64_t gb = base | scatter((unsigned)G[kStGeoTlo + (t & 15u)] | G[kStGeoThi + (t >> 4)]);
 				uint64_t go[kStRB];
 #pragma unroll
 				for(unsigned i = 0; i < kStRB; ++i) go[i] = scatter(1u << g.rbit[st][i]);
@@ -1245,10 +1312,10 @@ __global__ void __launch_bounds__(kStThreads, 2) k_fused_stages(typename Vec2<R>
 					a[x] = v[r];
 				}
 			} else {
-				const unsigned jb = st_slot(jl, g.swz);
+				const unsigned jb = (unsigned)G[kStGeoSlo + (t & 15u)] ^ G[kStGeoShi + (t >> 4)];
 				unsigned ro[kStRB];
 #pragma unroll
-				for(unsigned i = 0; i < kStRB; ++i) ro[i] = st_slot(1u << g.rbit[st][i], g.swz);
+				for(unsigned i = 0; i < kStRB; ++i) ro[i] = G[kStGeoReg + i];
 #pragma unroll
 				for(unsigned r = 0; r < 16; ++r) {
 					unsigned x = jb;
@@ -1265,54 +1332,54 @@ __global__ void __launch_bounds__(kStThreads, 2) k_fused_stages(typename Vec2<R>
 	}
 }
 
+// Shared slot of local index j under the swizzle scol (XOR-linear).
+unsigned stage_slot(unsigned j, const uint8_t (&scol)[kStK]) {
+	unsigned x = j;
+	for(unsigned b = 3; b < kStK; ++b)
+		if((j >> b) & 1u) x ^= scol[b];
+	return x;
+}
+
 // A swizzle under which every stage's quarter-warp lanes (thread index bits
-// 0-2) move 8 distinct bank groups: over GF(2), the slot bits 0-2 that lane
-// bits flip must be independent.  Searched over three XOR sources.
+// 0-2) move 8 distinct 16-byte bank groups: over GF(2), the slot bits 0-2
+// that those three local bits flip must be independent.  Each local bit
+// b >= 3 flips slot bits scol[b]; searched depth-first.  None found: no
+// swizzle (correct, with some conflicts).
 void stage_swizzle(StageGeom &g) {
-	auto ok = [&](const uint8_t (&sw)[3]) {
+	uint8_t col[kStK] = {};
+	unsigned assigned = 0x7u;  // bits 0-2 flip themselves
+	auto vec = [&](unsigned b) { return b < 3 ? (1u << b) : (unsigned)col[b]; };
+	auto stages_ok = [&]() {
 		for(unsigned st = 0; st < g.nstages; ++st) {
-			unsigned vec[3];
-			for(unsigned l = 0; l < 3; ++l) {
-				const unsigned b = g.tbit[st][l];
-				unsigned v = b < 3 ? (1u << b) : 0u;
-				for(unsigned i = 0; i < 3; ++i)
-					if(sw[i] && sw[i] == b) v ^= 1u << i;
-				vec[l] = v;
-			}
-			// Independent iff no nonempty subset XORs to zero.
-			for(unsigned m = 1; m < 8; ++m) {
-				unsigned x = 0;
-				for(unsigned l = 0; l < 3; ++l)
-					if((m >> l) & 1u) x ^= vec[l];
-				if(!x) return false;
-			}
+			const unsigned b0 = g.tbit[st][0], b1 = g.tbit[st][1], b2 = g.tbit[st][2];
+			if(!((assigned >> b0) & (assigned >> b1) & (assigned >> b2) & 1u)) continue;
+			const unsigned v0 = vec(b0), v1 = vec(b1), v2 = vec(b2);
+			if(!v0 || !v1 || !v2 || v0 == v1 || v0 == v2 || v1 == v2 || (v0 ^ v1) == v2) return false;
 		}
 		return true;
 	};
-	uint8_t sw[3] = {0, 0, 0};
-	if(ok(sw)) {
-		std::memcpy(g.swz, sw, 3);
-		return;
-	}
-	for(unsigned a = 0; a < kStK; ++a)
-		for(unsigned b = 0; b < kStK; ++b)
-			for(unsigned c = 0; c < kStK; ++c) {
-				const unsigned v[3] = {a, b, c};
-				bool valid = true;
-				for(unsigned i = 0; i < 3; ++i) valid = valid && (v[i] == 0 || v[i] >= 3);
-				if(!valid) continue;
-				uint8_t t3[3] = {(uint8_t)a, (uint8_t)b, (uint8_t)c};
-				if(ok(t3)) {
-					std::memcpy(g.swz, t3, 3);
-					return;
-				}
-			}
-	std::memset(g.swz, 0, 3);  // none fits every stage: unswizzled (correct, with some conflicts)
+	static const uint8_t order[8] = {0, 1, 2, 4, 3, 5, 6, 7};
+	unsigned nodes = 0;
+	std::function<bool(unsigned)> dfs = [&](unsigned b) -> bool {
+		if(b == kStK) return true;
+		for(unsigned i = 0; i < 8; ++i) {
+			if(++nodes > 200000) return false;
+			col[b] = order[i];
+			assigned |= 1u << b;
+			if(stages_ok() && dfs(b + 1)) return true;
+			assigned &= ~(1u << b);
+		}
+		col[b] = 0;
+		return false;
+	};
+	if(!dfs(3)) std::memset(col, 0, sizeof(col));
+	std::memcpy(g.scol, col, sizeof(col));
 }
 
 // The stage plan of an exact pass, when its program is Hadamards and H-chains
 // on distinct local bits of a 12-bit tile; false otherwise (k_fused runs it).
-bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phases, std::vector<uint64_t> &lbits) {
+// Fills the per-op thread-mask tables (kStTabWords words per op).
+bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phases, std::vector<uint64_t> &tab) {
 	if(pass.K != kStK || pass.ops.empty() || pass.ops.size() > kStMaxOps) return false;
 	g = StageGeom{};
 	g.n = pass.n;
@@ -1328,6 +1395,10 @@ bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phas
 		seen |= 1u << op.lt;
 		const unsigned lc = op.kind == kFHChain ? op.lc : 0u;
 		if(lc > 64) return false;
+		for(unsigned e = 0; e < lc; ++e) {
+			const int l = pass.chain[op.tab + e].local;
+			if(l >= (int)kStK || l == (int)op.lt) return false;
+		}
 		maxlc = std::max(maxlc, lc);
 		nent += lc;
 	}
@@ -1350,53 +1421,112 @@ bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phas
 		++g.st_count[g.nstages - 1];
 	}
 	for(unsigned st = 0; st < g.nstages; ++st) {
+		const bool edge = st == 0 || st + 1 == g.nstages;  // reads or writes HBM
+		// How many of the stage's chain entries each local bit controls.
+		unsigned cost[kStK] = {};
+		for(unsigned k = g.st_first[st]; k < g.st_first[st] + g.st_count[st]; ++k) {
+			const FusedOp &op = pass.ops[k];
+			const unsigned lc = op.kind == kFHChain ? op.lc : 0u;
+			for(unsigned e = 0; e < lc; ++e)
+				if(pass.chain[op.tab + e].local >= 0) ++cost[pass.chain[op.tab + e].local];
+		}
 		std::vector<unsigned> &R = regs[st];
-		// Filler register bits: high local bits first (local bits 0-2 stay thread bits:
-		// a quarter-warp then reads 8 consecutive 16-byte slots, no bank conflict).
-		for(int b = (int)kStK - 1; b >= 0 && R.size() < kStRB; --b)
-			if(std::find(R.begin(), R.end(), (unsigned)b) == R.end()) R.push_back((unsigned)b);
+		auto in = [](const std::vector<unsigned> &v, unsigned b) { return std::find(v.begin(), v.end(), b) != v.end(); };
+		// In a stage that reads or writes HBM, the lowest local bits (global
+		// bits 0-2) stay quarter-warp lanes: each warp access then covers whole
+		// 128-byte lines.
+		const unsigned low = edge ? std::min(g.m, 3u) : 0u;
+		// Filler register bits: the most frequent controls; on a tie, the high
+		// local bits.
+		while(R.size() < kStRB) {
+			int best = -1;
+			for(int b = (int)kStK - 1; b >= 0; --b) {
+				if(in(R, (unsigned)b) || (unsigned)b < low) continue;
+				if(best < 0 || cost[b] > cost[best]) best = b;
+			}
+			R.push_back((unsigned)best);
+		}
 		uint32_t rset = 0;
 		for(unsigned i = 0; i < kStRB; ++i) {
 			g.rbit[st][i] = (uint8_t)R[i];
 			rset |= 1u << R[i];
 		}
-		unsigned kk = 0;
+		// Lanes: those low bits first (ascending), then the least frequent
+		// controls (ascending on a tie); the warp bits take the rest.
+		std::vector<unsigned> rest;
 		for(unsigned b = 0; b < kStK; ++b)
-			if(!((rset >> b) & 1u)) g.tbit[st][kk++] = (uint8_t)b;
+			if(!((rset >> b) & 1u)) rest.push_back(b);
+		std::stable_sort(rest.begin(), rest.end(), [&](unsigned x, unsigned y) {
+			if((x < low) != (y < low)) return x < low;
+			if(cost[x] != cost[y]) return cost[x] < cost[y];
+			return x < y;
+		});
+		std::vector<unsigned> lanes(rest.begin(), rest.begin() + 5), warps(rest.begin() + 5, rest.end());
+		for(unsigned i = 0; i < 5; ++i) g.tbit[st][i] = (uint8_t)lanes[i];
+		for(unsigned i = 0; i < 3; ++i) g.tbit[st][5 + i] = (uint8_t)warps[i];
+	}
+	stage_swizzle(g);
+	for(unsigned st = 0; st < g.nstages; ++st) {
 		for(unsigned x = 0; x < 16; ++x) {
 			unsigned lo = 0, hi = 0;
 			for(unsigned i = 0; i < 4; ++i) {
 				if((x >> i) & 1u) lo |= 1u << g.tbit[st][i];
 				if((x >> i) & 1u) hi |= 1u << g.tbit[st][4 + i];
 			}
-			g.tlo[st][x] = (uint16_t)lo;
-			g.thi[st][x] = (uint16_t)hi;
+			g.geo[st][kStGeoTlo + x] = (uint16_t)lo;
+			g.geo[st][kStGeoThi + x] = (uint16_t)hi;
+			g.geo[st][kStGeoSlo + x] = (uint16_t)stage_slot(lo, g.scol);
+			g.geo[st][kStGeoShi + x] = (uint16_t)stage_slot(hi, g.scol);
 		}
+		for(unsigned i = 0; i < kStRB; ++i) g.geo[st][kStGeoReg + i] = (uint16_t)stage_slot(1u << g.rbit[st][i], g.scol);
 	}
 	phases.clear();
-	lbits.assign((size_t)g.nops * kStK, 0ull);
+	tab.assign((size_t)g.nops * kStTabWords, 0ull);
 	for(unsigned k = 0; k < g.nops; ++k) {
 		const FusedOp &op = pass.ops[k];
 		const unsigned lc = op.kind == kFHChain ? op.lc : 0u;
 		g.op_tab[k] = (uint16_t)phases.size();
 		g.op_lc[k] = (uint16_t)lc;
-		// The op's stage registers: entries after the last one they control are uniform per thread.
 		unsigned st = 0;
 		while(st + 1 < g.nstages && g.st_first[st + 1] <= k) ++st;
+		uint64_t tb[kStTB] = {}, rm[kStRB] = {};
 		unsigned split = 0;
 		for(unsigned e = 0; e < lc; ++e) {
 			const ChainEntry &ce = pass.chain[op.tab + e];
 			phases.push_back(double2{ce.cr, ce.ci});
-			if(ce.local >= 0) {
-				lbits[(size_t)k * kStK + ce.local] |= 1ull << (63 - e);
-				for(unsigned i = 0; i < kStRB; ++i)
-					if(g.rbit[st][i] == (unsigned)ce.local) split = e + 1;
-			}
+			if(ce.local < 0) continue;
+			const uint64_t bit = 1ull << (63 - e);
+			bool reg = false;
+			for(unsigned i = 0; i < kStRB; ++i)
+				if(g.rbit[st][i] == (unsigned)ce.local) {
+					rm[i] |= bit;
+					reg = true;
+					split = e + 1;
+				}
+			if(!reg)
+				for(unsigned i = 0; i < kStTB; ++i)
+					if(g.tbit[st][i] == (unsigned)ce.local) tb[i] |= bit;
 		}
 		g.op_split[k] = (uint8_t)split;
+		uint64_t *T = tab.data() + (size_t)k * kStTabWords;
+		uint64_t lo_all = 0;
+		for(unsigned x = 0; x < 16; ++x) {
+			uint64_t lo = 0, hi = 0;
+			for(unsigned i = 0; i < 4; ++i) {
+				if((x >> i) & 1u) lo |= tb[i];
+				if((x >> i) & 1u) hi |= tb[4 + i];
+			}
+			T[kStTabLo + x] = lo;
+			T[kStTabHi + x] = hi;
+			lo_all |= lo;
+		}
+		for(unsigned w = 0; w < kStThreads / 32; ++w) T[kStTabWarp + w] = lo_all | T[kStTabHi + 2 * w] | T[kStTabHi + 2 * w + 1];
+		for(unsigned i = 0; i < kStRB; ++i) {
+			T[kStTabReg + i] = rm[i];
+			T[kStTabRegAll] |= rm[i];
+		}
 	}
 	g.nentries = (unsigned)phases.size();
-	stage_swizzle(g);
 	return true;
 }
 
@@ -1404,8 +1534,8 @@ template <typename R>
 bool run_fused_stages(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_prog, size_t &dev_prog_bytes) {
 	StageGeom g;
 	std::vector<double2> phases;
-	std::vector<uint64_t> lbits;
-	if(!plan_stages(pass, g, phases, lbits)) return false;
+	std::vector<uint64_t> tab;
+	if(!plan_stages(pass, g, phases, tab)) return false;
 	g.ntiles = 1ull << (pass.n - kStK);
 	g.o_begin = 0;
 	if(pass.tile_end) {
@@ -1413,12 +1543,10 @@ bool run_fused_stages(const LaunchCtx &c, void *a, const FusedPass &pass, void *
 		g.o_begin = pass.tile_begin;
 		g.ntiles = pass.tile_end;
 	}
-	const size_t ops_bytes = pass.ops.size() * sizeof(FusedOp);
-	const size_t ch_off = (ops_bytes + 255) & ~size_t(255);
 	const size_t ch_bytes = std::max<size_t>(32, pass.chain.size() * sizeof(ChainEntry));
-	const size_t ph_off = (ch_off + ch_bytes + 255) & ~size_t(255);
-	const size_t lb_off = (ph_off + std::max<size_t>(16, phases.size() * sizeof(double2)) + 255) & ~size_t(255);
-	const size_t need = lb_off + lbits.size() * sizeof(uint64_t);
+	const size_t ph_off = (ch_bytes + 255) & ~size_t(255);
+	const size_t tab_off = (ph_off + std::max<size_t>(16, phases.size() * sizeof(double2)) + 255) & ~size_t(255);
+	const size_t need = tab_off + tab.size() * sizeof(uint64_t);
 	if(need > dev_prog_bytes) {
 		if(dev_prog) {
 			check_cuda(cudaStreamSynchronize(c.stream), "fused program sync");
@@ -1433,24 +1561,20 @@ bool run_fused_stages(const LaunchCtx &c, void *a, const FusedPass &pass, void *
 		dev_prog_bytes = need * 2;
 	}
 	std::vector<unsigned char> host(need, 0);
-	std::memcpy(host.data(), pass.ops.data(), ops_bytes);
-	if(!pass.chain.empty()) std::memcpy(host.data() + ch_off, pass.chain.data(), pass.chain.size() * sizeof(ChainEntry));
+	if(!pass.chain.empty()) std::memcpy(host.data(), pass.chain.data(), pass.chain.size() * sizeof(ChainEntry));
 	if(!phases.empty()) std::memcpy(host.data() + ph_off, phases.data(), phases.size() * sizeof(double2));
-	std::memcpy(host.data() + lb_off, lbits.data(), lbits.size() * sizeof(uint64_t));
+	std::memcpy(host.data() + tab_off, tab.data(), tab.size() * sizeof(uint64_t));
 	upload_async(c, dev_prog, host.data(), need, "fused program upload");
 	unsigned char *dp = static_cast<unsigned char *>(dev_prog);
-	auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };  // the kernel's region layout
-	const size_t smem = (sizeof(typename Vec2<R>::type) << kStK) + a16(sizeof(uint64_t) << (kStK - g.m)) +
-	                    a16(lbits.size() * sizeof(uint64_t)) + phases.size() * sizeof(double2) + phases.size();
+	const size_t smem = stage_smem_layout(sizeof(typename Vec2<R>::type), g.m, g.nops, g.nentries, g.nstages).total;
 	auto kern = g.narrow ? k_fused_stages<R, true> : k_fused_stages<R, false>;
 	check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "stage smem");
 	int per_sm = 1;
 	check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStThreads, smem), "stage occupancy");
 	const uint64_t grid = std::min<uint64_t>(g.ntiles - g.o_begin, (uint64_t)c.num_sms * std::max(1, per_sm));
 	kern<<<(unsigned)grid, kStThreads, smem, c.stream>>>(
-		static_cast<typename Vec2<R>::type *>(a), g, reinterpret_cast<const FusedOp *>(dp),
-		reinterpret_cast<const ChainEntry *>(dp + ch_off), reinterpret_cast<const double2 *>(dp + ph_off),
-		reinterpret_cast<const uint64_t *>(dp + lb_off));
+		static_cast<typename Vec2<R>::type *>(a), g, reinterpret_cast<const ChainEntry *>(dp),
+		reinterpret_cast<const double2 *>(dp + ph_off), reinterpret_cast<const uint64_t *>(dp + tab_off));
 	after_launch(c, "fused stage pass");
 	return true;
 }
