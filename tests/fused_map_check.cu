@@ -153,9 +153,10 @@ static void check_stages(const char *name, const FusedPass &p) {
 		std::vector<int> seen(T, 0);
 		for(unsigned t = 0; t < kStThreads; ++t) {
 			const unsigned jl = (unsigned)g.geo[st][kStGeoTlo + (t & 15u)] | g.geo[st][kStGeoThi + (t >> 4)];
-			unsigned want = 0;
+			unsigned col[kStTB], want = 0;
+			stage_thread_columns(g, st, col);
 			for(unsigned i = 0; i < kStTB; ++i)
-				if((t >> i) & 1u) want |= 1u << g.tbit[st][i];
+				if((t >> i) & 1u) want ^= col[i];
 			EXPECT(jl == want, "%s stage %u: local base of thread %u", name, st, t);
 			const unsigned jb = (unsigned)g.geo[st][kStGeoSlo + (t & 15u)] ^ g.geo[st][kStGeoShi + (t >> 4)];
 			for(unsigned r = 0; r < 16; ++r) {
@@ -194,7 +195,7 @@ static void check_stages(const char *name, const FusedPass &p) {
 			const unsigned split = g.op_split[k];
 			const uint64_t post = split ? ~(~0ull << (64 - split)) : ~0ull;
 			EXPECT((rall & post) == 0, "%s op %u: register control after the split", name, k);
-			double issued = 0.0, needed = 0.0;
+			double issued = 0.0, needed = 0.0, sub[4] = {};
 			for(unsigned w = 0; w < kStThreads / 32; ++w) {
 				uint64_t wu = 0;
 				for(unsigned l = 0; l < 32; ++l) {
@@ -222,7 +223,11 @@ static void check_stages(const char *name, const FusedPass &p) {
 				}
 				EXPECT(wu == Tb[kStTabWarp + w], "%s op %u: warp %u union", name, k, w);
 				issued += 32.0 * 8.0 * (double)__builtin_popcountll(wu & ~rall);
+				sub[w % 4] += (double)__builtin_popcountll(wu & ~rall);
 			}
+			// The four sub-partitions issue the same thread-controlled products.
+			EXPECT(sub[0] == sub[1] && sub[0] == sub[2] && sub[0] == sub[3], "%s op %u: sub-partitions %.0f %.0f %.0f %.0f",
+			       name, k, sub[0], sub[1], sub[2], sub[3]);
 			std::printf("stage %s op %u stage %u lt %u pairs %u issued %.0f needed %.0f\n", name, k, st, op.lt, T / 2, issued,
 			            needed);
 		}

@@ -1376,6 +1376,17 @@ void stage_swizzle(StageGeom &g) {
 	std::memcpy(g.scol, col, sizeof(col));
 }
 
+// Local offset flipped by each thread index bit of stage st: the lane bits
+// and warp bits 0-1 (which pick the SM sub-partition) flip one local bit
+// each, warp bit 2 flips all three warp-bit locals.  Warps w and w + 4 then
+// share a sub-partition with complementary warp-bit controls, so that every
+// sub-partition gets the same products whichever of those bits control
+// chain entries.
+void stage_thread_columns(const StageGeom &g, unsigned st, unsigned (&col)[kStTB]) {
+	for(unsigned i = 0; i < kStTB; ++i) col[i] = 1u << g.tbit[st][i];
+	col[7] = (1u << g.tbit[st][5]) | (1u << g.tbit[st][6]) | (1u << g.tbit[st][7]);
+}
+
 // The stage plan of an exact pass, when its program is Hadamards and H-chains
 // on distinct local bits of a 12-bit tile; false otherwise (k_fused runs it).
 // Fills the per-op thread-mask tables (kStTabWords words per op).
@@ -1467,11 +1478,13 @@ bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phas
 	}
 	stage_swizzle(g);
 	for(unsigned st = 0; st < g.nstages; ++st) {
+		unsigned col[kStTB];
+		stage_thread_columns(g, st, col);
 		for(unsigned x = 0; x < 16; ++x) {
 			unsigned lo = 0, hi = 0;
 			for(unsigned i = 0; i < 4; ++i) {
-				if((x >> i) & 1u) lo |= 1u << g.tbit[st][i];
-				if((x >> i) & 1u) hi |= 1u << g.tbit[st][4 + i];
+				if((x >> i) & 1u) lo ^= col[i];
+				if((x >> i) & 1u) hi ^= col[4 + i];
 			}
 			g.geo[st][kStGeoTlo + x] = (uint16_t)lo;
 			g.geo[st][kStGeoThi + x] = (uint16_t)hi;
@@ -1489,7 +1502,8 @@ bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phas
 		g.op_lc[k] = (uint16_t)lc;
 		unsigned st = 0;
 		while(st + 1 < g.nstages && g.st_first[st + 1] <= k) ++st;
-		uint64_t tb[kStTB] = {}, rm[kStRB] = {};
+		uint64_t *T = tab.data() + (size_t)k * kStTabWords;
+		uint64_t rm[kStRB] = {};
 		unsigned split = 0;
 		for(unsigned e = 0; e < lc; ++e) {
 			const ChainEntry &ce = pass.chain[op.tab + e];
@@ -1503,23 +1517,16 @@ bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phas
 					reg = true;
 					split = e + 1;
 				}
-			if(!reg)
-				for(unsigned i = 0; i < kStTB; ++i)
-					if(g.tbit[st][i] == (unsigned)ce.local) tb[i] |= bit;
+			if(reg) continue;
+			// A thread control: set for the nibbles whose local offset has it.
+			for(unsigned x = 0; x < 16; ++x) {
+				if((g.geo[st][kStGeoTlo + x] >> ce.local) & 1u) T[kStTabLo + x] |= bit;
+				if((g.geo[st][kStGeoThi + x] >> ce.local) & 1u) T[kStTabHi + x] |= bit;
+			}
 		}
 		g.op_split[k] = (uint8_t)split;
-		uint64_t *T = tab.data() + (size_t)k * kStTabWords;
 		uint64_t lo_all = 0;
-		for(unsigned x = 0; x < 16; ++x) {
-			uint64_t lo = 0, hi = 0;
-			for(unsigned i = 0; i < 4; ++i) {
-				if((x >> i) & 1u) lo |= tb[i];
-				if((x >> i) & 1u) hi |= tb[4 + i];
-			}
-			T[kStTabLo + x] = lo;
-			T[kStTabHi + x] = hi;
-			lo_all |= lo;
-		}
+		for(unsigned x = 0; x < 16; ++x) lo_all |= T[kStTabLo + x];
 		for(unsigned w = 0; w < kStThreads / 32; ++w) T[kStTabWarp + w] = lo_all | T[kStTabHi + 2 * w] | T[kStTabHi + 2 * w + 1];
 		for(unsigned i = 0; i < kStRB; ++i) {
 			T[kStTabReg + i] = rm[i];
