@@ -55,7 +55,8 @@ between steps.
           kinds: Hadamards, controlled phases on near and far qubits, swaps),
           timed by the reference's Simulator.
 
-roofline: the plain form's dominant kernel k_fused<double> is bound by FP64
+roofline: the plain form's dominant kernel k_fused_stages<double> (register
+stages of an exact pass of Hadamards and H-chains) is bound by FP64
 instruction issue, not HBM: every controlled phase is its own rounded complex
 product in the reference's operation order (4 DMUL + 2 DADD, no FMA), and a
 Hadamard butterfly is 4 FP64 operations per amplitude.  `achieved` is the
@@ -702,7 +703,7 @@ def run_ours(args):
         sm_mhz = clk.get("sm_mhz") or 1965.0
         fp64_peak = NUM_SMS * FP64_LANES_PER_SM * sm_mhz * 1e6 / 1e12
         achieved = fp64_per_launch / (avg_ms / 1e3) / 1e12
-        roofline = {"bound": "fp64", "kernel": "k_fused<double> (fused multi-gate pass, exact)", "achieved": achieved,
+        roofline = {"bound": "fp64", "kernel": "k_fused_stages<double> (exact pass of Hadamards and H-chains)", "achieved": achieved,
                     "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                     "peak_source": f"nominal FP64 issue rate: {NUM_SMS} SMs x {FP64_LANES_PER_SM} lanes x {sm_mhz:.0f} MHz "
                                    f"(median SM clock sampled in the timed region)",

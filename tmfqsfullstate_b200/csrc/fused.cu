@@ -67,12 +67,9 @@ struct ChainMap {
 };
 constexpr uint64_t kNoChainMap = ~0ull;
 
-#ifndef TMFQS_CHAIN_PAIRS
-#define TMFQS_CHAIN_PAIRS 4
-#endif
 // Butterflies per thread in a mapped H-chain op: independent chains of
 // dependent products that hide each other's latency.
-constexpr unsigned kChainPairs = TMFQS_CHAIN_PAIRS;
+constexpr unsigned kChainPairs = 4;
 
 // Chain products over one 32-entry word of a warp-uniform mask `mw` (the
 // union of the masks of all lanes and pairs; entry e = bit 31 - e of the
@@ -119,11 +116,8 @@ __device__ __forceinline__ bool butterfly(typename Vec2<R>::type &x, typename Ve
 	return true;
 }
 
-#ifndef TMFQS_FUSED_MIN_BLOCKS
-#define TMFQS_FUSED_MIN_BLOCKS 3
-#endif
 template <typename R>
-__global__ void __launch_bounds__(kFusedThreads, TMFQS_FUSED_MIN_BLOCKS) k_fused(typename Vec2<R>::type *a, FusedGeom g, const FusedOp *ops,
+__global__ void __launch_bounds__(kFusedThreads, 3) k_fused(typename Vec2<R>::type *a, FusedGeom g, const FusedOp *ops,
                                                             const ChainEntry *chain, const ChainMap *maps) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ unsigned char smem_raw[];
@@ -1272,6 +1266,17 @@ __global__ void __launch_bounds__(kStThreads, 2) k_fused_stages(typename Vec2<R>
 					for(unsigned i = 0; i < kStRB; ++i)
 						if((r >> i) & 1u) x |= go[i];
 					v[r] = a[x];
+				}
+				// The CTA's next tile into L2 while this one is transformed: its
+				// 512 runs of 8 contiguous amplitudes (local bits 0-2 are global
+				// bits 0-2), two per thread.
+				const uint64_t on = o + gridDim.x;
+				if(g.m >= 3 && on < g.ntiles) {
+					uint64_t nb = on;
+					for(unsigned i = 0; i < kStK; ++i) nb = insert0(nb, g.lpos[i]);
+#pragma unroll
+					for(unsigned h = 0; h < 2; ++h)
+						asm volatile("prefetch.global.L2 [%0];" ::"l"(a + (nb | scatter((t + h * kStThreads) << 3))));
 				}
 			} else {
 				const unsigned jb = (unsigned)G[kStGeoSlo + (t & 15u)] ^ G[kStGeoShi + (t >> 4)];

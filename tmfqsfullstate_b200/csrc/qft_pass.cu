@@ -349,10 +349,25 @@ __device__ __forceinline__ void qft_tail(const V *tile, V *dst, unsigned T, unsi
 		V out[E];
 #pragma unroll
 		for(int r = 0; r < (int)E; ++r) out[brev_bits(r, D)] = vscale(v[r], s);
-		if constexpr(sizeof(V) == 8) {
+		// 32-byte stores where a group spans whole sectors (sm_100 vector
+		// width): a lane then writes full sectors, not halves.
+		if constexpr(sizeof(V) == 8 && E >= 4) {
+#pragma unroll
+			for(unsigned e = 0; e < E; e += 4)
+				asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(dst + j + e), "f"(out[e].x),
+				             "f"(out[e].y), "f"(out[e + 1].x), "f"(out[e + 1].y), "f"(out[e + 2].x), "f"(out[e + 2].y),
+				             "f"(out[e + 3].x), "f"(out[e + 3].y)
+				             : "memory");
+		} else if constexpr(sizeof(V) == 8) {
 #pragma unroll
 			for(unsigned e = 0; e < E; e += 2)
 				*reinterpret_cast<float4 *>(dst + j + e) = make_float4(out[e].x, out[e].y, out[e + 1].x, out[e + 1].y);
+		} else if constexpr(E >= 2) {
+#pragma unroll
+			for(unsigned e = 0; e < E; e += 2)
+				asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(dst + j + e), "d"((double)out[e].x),
+				             "d"((double)out[e].y), "d"((double)out[e + 1].x), "d"((double)out[e + 1].y)
+				             : "memory");
 		} else {
 #pragma unroll
 			for(unsigned e = 0; e < E; ++e) dst[j + e] = out[e];
