@@ -215,6 +215,24 @@ def test_fused_qft_bitexact(gpu, n):
     assert st["kernel_launches"] > 0
 
 
+@pytest.mark.parametrize("kind", ["sparse", "pattern", "basis"])
+def test_fused_qft_zero_inputs_bitexact(gpu, kind):
+    """QFT-16 through the register-stage pass on inputs with exact zeros (all-zero
+    pairs skipped by whole warps, zero amplitudes taking no phase), compared bit
+    for bit, signs of zeros included."""
+    n = 16
+    if kind == "sparse":
+        a = rand_state(n, 77, zeros=0.7)
+    else:
+        a = np.zeros(2 << n)
+        if kind == "pattern":
+            a[0::2 << 4] = 2.0 ** (-(n - 4) / 2)  # uniform over the multiples of 2^4
+        else:
+            a[2 * 5] = 1.0
+    got, ref = ops_equal_run(gpu, n, a, tq.qft_ops(n))
+    assert_same(got.view(np.uint64), ref.view(np.uint64), f"QFT-16 {kind} (bits)")
+
+
 @pytest.mark.parametrize("seed", range(6))
 def test_fused_random_circuits_bitexact(gpu, seed):
     rng = np.random.default_rng(seed)

@@ -523,6 +523,12 @@ __device__ __forceinline__ uint64_t compress_outer(uint64_t x, const PermGeom &g
 	return x;
 }
 
+// One 16-byte granule: two complex64 or one complex128 amplitude.
+__device__ __forceinline__ void store_granule(float2 *p, const float2 (&y)[2]) {
+	*reinterpret_cast<float4 *>(p) = make_float4(y[0].x, y[0].y, y[1].x, y[1].y);
+}
+__device__ __forceinline__ void store_granule(double2 *p, const double2 (&y)[1]) { *p = y[0]; }
+
 template <typename R>
 __global__ void __launch_bounds__(kPermThreads) k_bit_perm(typename Vec2<R>::type *a, PermGeom g) {
 	typedef typename Vec2<R>::type V;
@@ -630,17 +636,16 @@ __global__ void __launch_bounds__(kPermThreads) k_bit_perm(typename Vec2<R>::typ
 #pragma unroll
 		for(unsigned i = 0; i < kPermGranules; ++i) {
 			if(!gv[i]) continue;
-			float4 wa, wb;
-			V *ya = reinterpret_cast<V *>(&wa), *yb = reinterpret_cast<V *>(&wb);
+			V ya[G], yb[G];
 #pragma unroll
 			for(unsigned e = 0; e < G; ++e) {
 				ya[e] = A[src[i][e]];
 				if(pair) yb[e] = B[src[i][e]];
 			}
-			*reinterpret_cast<float4 *>(a + (cur.pbase | goff[i])) = wa;
-			if(pair) *reinterpret_cast<float4 *>(a + (cur.base | goff[i])) = wb;
+			store_granule(a + (cur.pbase | goff[i]), ya);
+			if(pair) store_granule(a + (cur.base | goff[i]), yb);
 		}
-		__syncthreads();
+		__syncthreads();  // every read of this buffer is done before it is refilled
 		cur = nxt;
 		sel ^= 1u;
 	}
@@ -1125,12 +1130,17 @@ template <typename R, unsigned I, bool NARROW>
 __device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R inv, bool chain, unsigned k,
                                              const StageGeom &g, const uint64_t *tab, const double2 *ph,
                                              const uint8_t *ebit, uint64_t base, unsigned t) {
-	unsigned pz = 0;  // some pair of this thread is all zero
+	unsigned pz = 0, pall = 1;  // some / every pair of this thread is all zero
 #pragma unroll
 	for(unsigned p = 0; p < 8; ++p) {
 		const unsigned r1 = st_r1<I>(p), r0 = r1 ^ (1u << I);
-		pz |= (st_bits_nonsign(v[r0]) | st_bits_nonsign(v[r1])) == 0u;
+		const unsigned z = (st_bits_nonsign(v[r0]) | st_bits_nonsign(v[r1])) == 0u;
+		pz |= z;
+		pall &= z;
 	}
+	// A warp whose pairs are all zero has nothing to do for this op: zero
+	// pairs are left as they are and zero amplitudes take no phase.
+	if(__all_sync(0xffffffffu, pall)) return;
 	if(__any_sync(0xffffffffu, pz)) {
 #pragma unroll
 		for(unsigned p = 0; p < 8; ++p) {
@@ -1146,12 +1156,14 @@ __device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R 
 	}
 	if(!chain) return;
 	bool nz[8];
-	bool mine = true;
+	bool mine = true, some = false;
 #pragma unroll
 	for(unsigned p = 0; p < 8; ++p) {
 		nz[p] = st_bits_nonsign(v[st_r1<I>(p)]) != 0u;
 		mine = mine && nz[p];
+		some = some || nz[p];
 	}
+	if(!__any_sync(0xffffffffu, some)) return;  // no |1> output of the warp takes a phase
 	const bool all = __all_sync(0xffffffffu, mine);
 	// The entries whose control is an outer bit set in this tile (one lane per
 	// entry, the same in every warp).

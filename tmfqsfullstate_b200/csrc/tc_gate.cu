@@ -130,15 +130,26 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gate(float2 *a, TcGateGeom g,
 #pragma unroll
 		for(int c = 0; c < D; ++c) x[c] = a[gb0 + soff[c]];
 	}
+
 	for(; tile < g.ntiles && ok; tile += gridDim.x, phase ^= 1u) {
 		const uint64_t gb = group_base(tile), next = tile + gridDim.x;
+		// Four consecutive columns share a 16-byte chunk of the swizzled row:
+		// one 16-byte store each, so 8 consecutive rows fill the 8 chunks of a
+		// 128-byte line (no bank conflict).
 #pragma unroll
-		for(int c = 0; c < D; ++c) {
-			const float hr = tf32_hi(x[c].x), hi = tf32_hi(x[c].y);
-			*reinterpret_cast<float *>(ah + sw128(tid, c, kTcRows)) = hr;
-			*reinterpret_cast<float *>(ah + sw128(tid, D + c, kTcRows)) = hi;
-			*reinterpret_cast<float *>(al + sw128(tid, c, kTcRows)) = x[c].x - hr;
-			*reinterpret_cast<float *>(al + sw128(tid, D + c, kTcRows)) = x[c].y - hi;
+		for(int c = 0; c < D; c += 4) {
+			float hr[4], hi[4];
+#pragma unroll
+			for(int j = 0; j < 4; ++j) {
+				hr[j] = tf32_hi(x[c + j].x);
+				hi[j] = tf32_hi(x[c + j].y);
+			}
+			*reinterpret_cast<float4 *>(ah + sw128(tid, c, kTcRows)) = make_float4(hr[0], hr[1], hr[2], hr[3]);
+			*reinterpret_cast<float4 *>(ah + sw128(tid, D + c, kTcRows)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+			*reinterpret_cast<float4 *>(al + sw128(tid, c, kTcRows)) =
+				make_float4(x[c].x - hr[0], x[c + 1].x - hr[1], x[c + 2].x - hr[2], x[c + 3].x - hr[3]);
+			*reinterpret_cast<float4 *>(al + sw128(tid, D + c, kTcRows)) =
+				make_float4(x[c].y - hi[0], x[c + 1].y - hi[1], x[c + 2].y - hi[2], x[c + 3].y - hi[3]);
 		}
 		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 		__syncthreads();
