@@ -58,21 +58,34 @@ static FusedPass make(unsigned n, const std::vector<unsigned> &local, const std:
 	return p;
 }
 
+// A QFT segment, else a Walsh segment (Hadamards only), as launch_qft_pass
+// tries them; for a Walsh plan, every stage is marked and the tail (if any)
+// sits on the lowest bits.
 static void check(const char *name, const FusedPass &p) {
 	std::vector<unsigned> hb;
 	unsigned r0 = 0;
 	const bool seg = qft_segment(p, hb, r0);
+	bool walsh = false;
+	if(!seg) {
+		walsh = walsh_segment(p, hb);
+		r0 = p.n;
+	}
 	int planned = -1;
-	unsigned nstages = 0;
+	unsigned nstages = 0, marked = 0, tail = 0;
 	double scale = 0.0;
-	if(seg) {
+	if(seg || walsh) {
 		QftGeom g{};
-		planned = plan_qft(p, hb, r0, 8, 5, g) ? 1 : 0;
+		planned = plan_qft(p, hb, r0, 8, 5, g, walsh) ? 1 : 0;
 		nstages = g.nstages;
 		scale = g.scale;
+		for(unsigned s = 0; s < g.nstages; ++s) {
+			marked += g.st[s].walsh ? 1u : 0u;
+			if(walsh && g.st[s].wmask) planned = 0;  // a Walsh stage takes no twiddle
+		}
+		tail = g.nstages ? g.st[g.nstages - 1].tail : 0u;
 	}
-	std::printf("case %s segment %d hb %zu r0 %u planned %d nstages %u scale %.17g\n", name, (int)seg, hb.size(), seg ? r0 : 0u,
-	            planned, nstages, scale);
+	std::printf("case %s segment %d hb %zu r0 %u planned %d nstages %u scale %.17g walsh %d marked %u tail %u\n", name,
+	            (int)seg, hb.size(), seg ? r0 : 0u, planned, nstages, scale, (int)walsh, marked, tail);
 }
 
 static std::vector<unsigned> range(unsigned lo, unsigned hi) {  // [lo, hi)
@@ -98,5 +111,12 @@ int main() {
 	check("dropped_phase", make(28, range(0, 13), down(11, 0), 0, true));
 	check("wrong_angle", make(28, range(0, 13), down(11, 0), 0, false, true));
 	check("sub_register", make(20, range(0, 13), down(12, 6), 3));
+	// Hadamards only: the top bits of a 24-qubit state, the 13 lowest bits
+	// (last stage fused into the copy-out), and scattered bits.
+	std::vector<unsigned> wl = range(0, 5), wt = range(16, 24);
+	wl.insert(wl.end(), wt.begin(), wt.end());
+	check("walsh_top", make(24, wl, down(23, 16), 0, false, false, true));
+	check("walsh_low", make(24, range(0, 13), down(12, 0), 0, false, false, true));
+	check("walsh_scattered", make(24, range(0, 13), {3, 11, 7, 9}, 0, false, false, true));
 	return 0;
 }

@@ -2,7 +2,8 @@
 
 Passes that are a segment of the QFT ladder (Hadamards on consecutive
 descending bits, each followed by the phases pi/2^(b-c) with every lower bit c
-of the register) run as k_qft_pass: register stages of up to 5 (complex64) or
+of the register), and passes of Hadamards only (Walsh segments), run as
+k_qft_pass: register stages of up to 5 (complex64) or
 4 (complex128) bits, per-thread and per-tile twiddle tables, a per-pass bank
 swizzle.  These cases reach its layouts: whole-register QFTs from one tile up
 (one pass, no outer bits) to several passes with outer bits between the local
@@ -57,10 +58,10 @@ def oracle(n, amps, ops):
     return r.amplitudes()
 
 
-def check(n, amps, ops, prec, **kw):
+def check(n, amps, ops, prec, expect_qft=True, **kw):
     want = oracle(n, amps, ops)
     got, st = run_gpu(n, amps, ops, prec, **kw)
-    assert st["qft_passes"] > 0, st
+    assert (st["qft_passes"] > 0) == expect_qft, st
     assert O.rel_l2(want, got) <= TOL[prec]
     ref, st0 = run_gpu(n, amps, ops, prec, qft_pass=False, **kw)
     assert st0["qft_passes"] == 0
@@ -115,8 +116,27 @@ def test_hadamard_runs_are_not_qft_segments(prec, chunk):
     assert O.rel_l2(oracle(n, a, ops), got) <= TOL[prec]
     layer = [tq.h(q) for q in range(n)]
     got, st = run_chunks(n, a, layer, prec, chunk)
-    assert st["qft_passes"] == 0
+    # They run as Walsh segments instead (butterflies only, no twiddles).
+    assert st["qft_passes"] > 0
     assert O.rel_l2(oracle(n, a, layer), got) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", [tq.FP64, tq.FP32])
+@pytest.mark.parametrize("bits", ["top", "low", "scattered", "all"])
+def test_walsh_pass(prec, bits):
+    """Hadamard-only passes through k_qft_pass's Walsh stages: the top 8
+    qubits, the 13 lowest index bits (last stage fused into the copy-out), and
+    a whole-register layer; against the oracle and the general radix pass.
+    Scattered qubits leave the tile's top local bits apart, which k_qft_pass's
+    copies need contiguous: that pass stays on k_radix."""
+    n = 22
+    qs = {"top": list(range(8)), "low": list(range(n - 13, n)), "scattered": [1, 4, 9, 15, 18, 20],
+          "all": list(range(n))}[bits]
+    ops = [tq.h(q) for q in qs]
+    rng = np.random.default_rng(len(qs))
+    a = rng.standard_normal(2 << n)
+    a /= np.linalg.norm(a)
+    check(n, a, ops, prec, expect_qft=bits != "scattered")
 
 
 @pytest.mark.parametrize("prec", [tq.FP64, tq.FP32])

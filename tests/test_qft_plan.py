@@ -1,6 +1,7 @@
 """The QFT segment recogniser and planner on the host (CPU only), through
-tests/qft_plan_check.cu: which passes run as QFT segments, their stage
-counts and their real scale (1/sqrt(2))^P."""
+tests/qft_plan_check.cu: which passes run as QFT segments or as Walsh
+segments (Hadamards only), their stage counts and their real scale
+(1/sqrt(2))^P."""
 import math
 import os
 import shutil
@@ -25,7 +26,8 @@ def cases(tmp_path_factory):
     for line in out.splitlines():
         f = line.split()
         res[f[1]] = {"segment": int(f[3]), "hb": int(f[5]), "r0": int(f[7]), "planned": int(f[9]),
-                     "nstages": int(f[11]), "scale": float(f[13])}
+                     "nstages": int(f[11]), "scale": float(f[13]), "walsh": int(f[15]), "marked": int(f[17]),
+                     "tail": int(f[19])}
     return res
 
 
@@ -47,3 +49,15 @@ def test_non_ladders_are_rejected(cases, name):
     """Hadamard runs without their phases, a chain missing a phase, and a
     wrong angle go to the general radix pass."""
     assert cases[name]["segment"] == 0
+
+
+@pytest.mark.parametrize("name,hadamards,stages,tail", [("walsh_top", 8, 2, 0), ("walsh_low", 13, 3, 1),
+                                                       ("walsh_scattered", 4, 1, 0), ("bare_run", 4, 1, 0)])
+def test_walsh_passes_are_planned(cases, name, hadamards, stages, tail):
+    """Hadamard-only passes are no QFT segment but plan as Walsh segments:
+    every stage marked, no twiddles, the scale (1/sqrt(2))^P, the lowest
+    bits' stage fused into the copy-out."""
+    c = cases[name]
+    assert c["segment"] == 0 and c["walsh"] == 1 and c["planned"] == 1
+    assert c["hb"] == hadamards and c["nstages"] == stages and c["marked"] == stages and c["tail"] == tail
+    assert math.isclose(c["scale"], 0.5 ** (hadamards / 2), rel_tol=1e-15)

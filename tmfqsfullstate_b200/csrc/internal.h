@@ -184,7 +184,9 @@ bool launch_radix_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &p
 // descending bits, each followed by the phases pi/2^(b-c) with every lower bit
 // c of the register) in the fast forms.  Returns false (nothing launched) when
 // the pass is not such a segment or its layout does not qualify.
-bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass);
+// A QFT segment pass (k_qft_pass); with allow_walsh also a pass of Hadamards
+// only.  False: the pass is neither (or does not fit the kernel's tiles).
+bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, bool allow_walsh);
 
 // ---------------------------------------------------------------------------
 // Adjoint gradient (adjoint.cu)

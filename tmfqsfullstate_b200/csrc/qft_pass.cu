@@ -59,6 +59,8 @@ struct QftStage {
 	uint32_t direct;      // last stage: results go straight to HBM (lanes run along >= 64-byte rows)
 	uint32_t top;         // register bit i is local bit kTop - 1 - i (the tile's top bits), unswizzled
 	uint32_t tail;        // last stage on the tile's lowest bits, fused into the copy-out (qft_tail)
+	uint32_t walsh;       // Hadamards only (a Walsh segment): butterflies, no phases
+	uint32_t pad_;
 	uint64_t wmask;       // the bits of W: [r0, lowest Hadamard bit of the stage)
 	uint64_t gstride[5];  // global element offset of register bit i
 };
@@ -191,7 +193,21 @@ __device__ __forceinline__ void apply_twiddle(V (&v)[1 << RB], const V (&f)[D], 
 
 // One stage on the tile in shared memory: the thread's 2^RB amplitudes are
 // read, transformed (ladder, twiddle, scale) and written back in place.
-template <typename V, int RB, int D, bool TW, bool SC, bool TOP>
+// Butterflies on register bits 0..D-1 (a Walsh-Hadamard stage), unscaled.
+template <typename V, int RB, int D>
+__device__ __forceinline__ void walsh_ladder(V (&v)[1 << RB]) {
+#pragma unroll
+	for(int i = 0; i < D; ++i) {
+#pragma unroll
+		for(int q = 0; q < (1 << (RB - 1)); ++q) {
+			const int lo = (1 << i) - 1;
+			const int r0 = ((q & ~lo) << 1) | (q & lo), r1 = r0 | (1 << i);
+			bfly2(v[r0], v[r1]);
+		}
+	}
+}
+
+template <typename V, int RB, int D, bool TW, bool SC, bool TOP, bool W = false>
 __device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
                                               const V *ot, typename Scalar<V>::type s, const RootTable &roots, V *gdst) {
 	// TOP: the register bits are the tile's top local bits in order, so the
@@ -209,7 +225,8 @@ __device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsign
 			if((r >> i) & 1) x ^= roff[i];
 		v[r] = TOP ? tile[pbase + x] : tile[x];
 	}
-	qft_stage<V, RB, D>(v, roots);
+	if constexpr(W) walsh_ladder<V, RB, D>(v);
+	else qft_stage<V, RB, D>(v, roots);
 	if constexpr(TW) {
 		V f[D];
 #pragma unroll
@@ -254,7 +271,10 @@ template <typename V, int RB, int D>
 __device__ __forceinline__ void qft_stage_flags(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
                                                 const V *ot, typename Scalar<V>::type s, const RootTable &roots, V *gdst) {
 	const bool tw = S.fl != kQftNone;
-	if(tw) {
+	if(S.walsh) {
+		if(S.scaled) qft_stage_run<V, RB, D, false, true, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, gdst);
+		else qft_stage_run<V, RB, D, false, false, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
+	} else if(tw) {
 		if(S.scaled) qft_stage_run<V, RB, D, true, true, false>(tile, S, pbase, frow, nthr, ot, s, roots, gdst);
 		else if(S.top) qft_stage_run<V, RB, D, true, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
 		else qft_stage_run<V, RB, D, true, false, false>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
@@ -320,7 +340,7 @@ __host__ __device__ constexpr int brev_bits(int r, int d) {
 // applies their ladder and the pass's scale, and stores them contiguously
 // (consecutive threads take consecutive groups).  Register bit i is local bit
 // D-1-i, so register r holds element brev(r).
-template <typename V, int D>
+template <typename V, int D, bool W>
 __device__ __forceinline__ void qft_tail(const V *tile, V *dst, unsigned T, unsigned tid, unsigned nthr, const QftGeom &g,
                                          typename Scalar<V>::type s) {
 	constexpr unsigned E = 1u << D;
@@ -345,7 +365,8 @@ __device__ __forceinline__ void qft_tail(const V *tile, V *dst, unsigned T, unsi
 		V v[E];
 #pragma unroll
 		for(int r = 0; r < (int)E; ++r) v[r] = in[brev_bits(r, D)];
-		qft_stage<V, D, D>(v, g.roots);
+		if constexpr(W) walsh_ladder<V, D, D>(v);
+		else qft_stage<V, D, D>(v, g.roots);
 		V out[E];
 #pragma unroll
 		for(int r = 0; r < (int)E; ++r) out[brev_bits(r, D)] = vscale(v[r], s);
@@ -438,7 +459,7 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 		if(st + 1 == g.nstages) slast = qft_scatter(g, jt);
 	}
 	const bool direct = sst[g.nstages - 1].direct != 0;
-	const bool tail = sst[g.nstages - 1].tail != 0;
+	const bool tail = sst[g.nstages - 1].tail != 0, wtail = sst[g.nstages - 1].walsh != 0;
 	const unsigned nrun = tail ? g.nstages - 1 : g.nstages;  // stages run through shared memory
 
 	const typename Scalar<V>::type s = (typename Scalar<V>::type)g.scale;
@@ -470,9 +491,12 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 		}
 		if(tail) {
 			switch(sst[g.nstages - 1].d) {
-				case 1: qft_tail<V, 1>(tile, a + tbase, T, tid, nthr, g, s); break;
-				case 2: qft_tail<V, 2>(tile, a + tbase, T, tid, nthr, g, s); break;
-				case 3: qft_tail<V, 3>(tile, a + tbase, T, tid, nthr, g, s); break;
+				case 1: wtail ? qft_tail<V, 1, true>(tile, a + tbase, T, tid, nthr, g, s)
+				              : qft_tail<V, 1, false>(tile, a + tbase, T, tid, nthr, g, s); break;
+				case 2: wtail ? qft_tail<V, 2, true>(tile, a + tbase, T, tid, nthr, g, s)
+				              : qft_tail<V, 2, false>(tile, a + tbase, T, tid, nthr, g, s); break;
+				case 3: wtail ? qft_tail<V, 3, true>(tile, a + tbase, T, tid, nthr, g, s)
+				              : qft_tail<V, 3, false>(tile, a + tbase, T, tid, nthr, g, s); break;
 				default: break;
 			}
 		} else if(!direct) {
@@ -541,6 +565,23 @@ bool qft_segment(const FusedPass &pass, std::vector<unsigned> &hb, unsigned &r0)
 	return hb.back() >= r0;
 }
 
+// Hadamards only, on two or more distinct local bits (a Walsh-Hadamard
+// segment: the Hadamards commute, so hb is any order of their bits; here
+// descending, as in a QFT segment).
+bool walsh_segment(const FusedPass &pass, std::vector<unsigned> &hb) {
+	hb.clear();
+	uint64_t seen = 0;
+	for(const FusedOp &f : pass.ops) {
+		if(f.kind != kFH || f.lt >= pass.K) return false;
+		const unsigned b = pass.lpos[f.lt];
+		if((seen >> b) & 1ull) return false;
+		seen |= 1ull << b;
+		hb.push_back(b);
+	}
+	std::sort(hb.begin(), hb.end(), [](unsigned x, unsigned y) { return x > y; });
+	return hb.size() >= 2;
+}
+
 inline unsigned insert_zeros(unsigned t, const uint32_t *sorted, int count) {
 	for(int i = 0; i < count; ++i) {
 		const unsigned b = sorted[i], lo = t & ((1u << b) - 1u);
@@ -561,7 +602,7 @@ struct Swizzle {
 
 // Plans the pass for storage values of vbytes bytes and RB register bits.
 bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r0, unsigned vbytes, unsigned RB,
-              QftGeom &g) {
+              QftGeom &g, bool walsh) {
 	const unsigned K = pass.K, n = pass.n, per16 = 16 / vbytes;
 	const unsigned lgran = RB - (per16 == 2 ? 1u : 0u);  // log2 of the granules per thread
 	if(K > 14 || K < RB + 5 || (1u << (K - RB)) > qft_max_threads(vbytes, (int)RB)) return false;
@@ -636,6 +677,7 @@ bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r
 			}
 		}
 		S.scaled = s + 1 == nst;
+		S.walsh = walsh;
 		for(unsigned i = 0; i < RB; ++i) S.gstride[i] = 1ull << pass.lpos[rbit[s][i]];
 		// Direct stores from the last stage when its lanes start with the lowest
 		// contiguous index bits: rows of at least 64 bytes per warp store.
@@ -750,10 +792,11 @@ bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r
 }
 
 template <typename R, int RB>
-bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r0) {
+bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r0,
+             bool walsh) {
 	typedef typename Vec2<R>::type V;
 	QftGeom g;
-	if(!c.err || !plan_qft(pass, hb, r0, (unsigned)sizeof(V), (unsigned)RB, g)) return false;
+	if(!c.err || !plan_qft(pass, hb, r0, (unsigned)sizeof(V), (unsigned)RB, g, walsh)) return false;
 	const unsigned nthr = 1u << (g.K - RB);
 	const size_t T = size_t(1) << g.K;
 	auto smem_for = [&](unsigned slots) {
@@ -776,15 +819,20 @@ bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass, const std::vect
 
 }  // namespace
 
-bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass) {
+bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, bool allow_walsh) {
 	std::vector<unsigned> hb;
 	unsigned r0 = 0;
-	if(!qft_segment(pass, hb, r0)) return false;
-	if(prec == TMFQS_FP64) return run_qft<double, 4>(c, a, pass, hb, r0);
+	bool walsh = false;
+	if(!qft_segment(pass, hb, r0)) {
+		if(!allow_walsh || !walsh_segment(pass, hb)) return false;
+		walsh = true;
+		r0 = pass.n;  // no phases: no twiddle range
+	}
+	if(prec == TMFQS_FP64) return run_qft<double, 4>(c, a, pass, hb, r0, walsh);
 	// complex64: 5-bit stages (256 threads).  4-bit stages with 512 threads
 	// measured the same at 28 and 30 qubits and 2% slower at 26 with one
 	// barrier per tile.
-	return run_qft<float, 5>(c, a, pass, hb, r0);
+	return run_qft<float, 5>(c, a, pass, hb, r0, walsh);
 }
 
 }  // namespace tqb
