@@ -1130,23 +1130,26 @@ template <typename R, unsigned I, bool NARROW>
 __device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R inv, bool chain, unsigned k,
                                              const StageGeom &g, const uint64_t *tab, const double2 *ph,
                                              const uint8_t *ebit, uint64_t base, unsigned t) {
-	unsigned pz = 0, pall = 1;  // some / every pair of this thread is all zero
+	unsigned pz = 0;  // some pair of this thread is all zero
 #pragma unroll
 	for(unsigned p = 0; p < 8; ++p) {
 		const unsigned r1 = st_r1<I>(p), r0 = r1 ^ (1u << I);
-		const unsigned z = (st_bits_nonsign(v[r0]) | st_bits_nonsign(v[r1])) == 0u;
-		pz |= z;
-		pall &= z;
+		pz |= (st_bits_nonsign(v[r0]) | st_bits_nonsign(v[r1])) == 0u;
 	}
-	// A warp whose pairs are all zero has nothing to do for this op: zero
-	// pairs are left as they are and zero amplitudes take no phase.
-	if(__all_sync(0xffffffffu, pall)) return;
-	if(__any_sync(0xffffffffu, pz)) {
+	const bool zeros = __any_sync(0xffffffffu, pz);  // the warp holds a zero pair (rare but for sparse states)
+	if(zeros) {
+		unsigned pall = 1;
 #pragma unroll
 		for(unsigned p = 0; p < 8; ++p) {
 			const unsigned r1 = st_r1<I>(p), r0 = r1 ^ (1u << I);
-			if((st_bits_nonsign(v[r0]) | st_bits_nonsign(v[r1])) != 0u) st_bfly<R>(v[r0], v[r1], inv);
+			if((st_bits_nonsign(v[r0]) | st_bits_nonsign(v[r1])) != 0u) {
+				st_bfly<R>(v[r0], v[r1], inv);
+				pall = 0;
+			}
 		}
+		// A warp whose pairs are all zero has nothing more to do for this op:
+		// zero pairs stay as they are and zero amplitudes take no phase.
+		if(__all_sync(0xffffffffu, pall)) return;
 	} else {
 #pragma unroll
 		for(unsigned p = 0; p < 8; ++p) {
@@ -1163,7 +1166,7 @@ __device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R 
 		mine = mine && nz[p];
 		some = some || nz[p];
 	}
-	if(!__any_sync(0xffffffffu, some)) return;  // no |1> output of the warp takes a phase
+	if(zeros && !__any_sync(0xffffffffu, some)) return;  // no |1> output of the warp takes a phase
 	const bool all = __all_sync(0xffffffffu, mine);
 	// The entries whose control is an outer bit set in this tile (one lane per
 	// entry, the same in every warp).
