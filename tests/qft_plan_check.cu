@@ -71,11 +71,11 @@ static void check(const char *name, const FusedPass &p) {
 		r0 = p.n;
 	}
 	int planned = -1;
-	unsigned nstages = 0, marked = 0, tail = 0;
+	unsigned nstages = 0, marked = 0, tail = 0, tma = 0, tdims = 0, tok = 1;
 	double scale = 0.0;
 	if(seg || walsh) {
 		QftGeom g{};
-		planned = plan_qft(p, hb, r0, 8, 5, g, walsh) ? 1 : 0;
+		planned = plan_qft(p, hb, r0, 8, 5, g, walsh, true) ? 1 : 0;
 		nstages = g.nstages;
 		scale = g.scale;
 		for(unsigned s = 0; s < g.nstages; ++s) {
@@ -83,9 +83,34 @@ static void check(const char *name, const FusedPass &p) {
 			if(walsh && g.st[s].wmask) planned = 0;  // a Walsh stage takes no twiddle
 		}
 		tail = g.nstages ? g.st[g.nstages - 1].tail : 0u;
+		tma = g.tma;
+		tdims = g.tma ? g.tma_dims : 0u;
+		if(g.tma) {
+			// The box enumerates the local index in order (ascending runs, the
+			// outer runs of box 1, strides 8 << first bit), and the copy's
+			// 128-byte swizzle (byte bits 4-6 ^= bits 7-9) is the pass's swizzle.
+			uint64_t elems = 1;
+			unsigned bit = 0, local = 0;
+			for(unsigned i = 0; i < g.tma_dims; ++i) {
+				if(g.tma_stride[i] != (8ull << bit) && i) tok = 0;
+				if(!g.tma_outer[i]) {
+					elems *= g.tma_box[i];
+					for(unsigned b = 0; b < g.tma_len[i]; ++b)
+						if(g.lpos[local++] != bit + b) tok = 0;
+				} else if(g.tma_box[i] != 1) {
+					tok = 0;
+				}
+				bit += g.tma_len[i];
+			}
+			if(elems != (1ull << g.K) || bit != p.n || g.tma_box[0] * 8 != 128) tok = 0;
+			for(unsigned j = 0; j < (1u << g.K); ++j) {
+				const unsigned byte = j * 8, tswz = byte ^ (((byte >> 7) & 7u) << 4);
+				if(tswz != qft_phys(g, j) * 8) tok = 0;
+			}
+		}
 	}
-	std::printf("case %s segment %d hb %zu r0 %u planned %d nstages %u scale %.17g walsh %d marked %u tail %u\n", name,
-	            (int)seg, hb.size(), seg ? r0 : 0u, planned, nstages, scale, (int)walsh, marked, tail);
+	std::printf("case %s segment %d hb %zu r0 %u planned %d nstages %u scale %.17g walsh %d marked %u tail %u tma %u dims %u tok %u\n",
+	            name, (int)seg, hb.size(), seg ? r0 : 0u, planned, nstages, scale, (int)walsh, marked, tail, tma, tdims, tok);
 }
 
 static std::vector<unsigned> range(unsigned lo, unsigned hi) {  // [lo, hi)

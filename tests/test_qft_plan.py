@@ -27,7 +27,7 @@ def cases(tmp_path_factory):
         f = line.split()
         res[f[1]] = {"segment": int(f[3]), "hb": int(f[5]), "r0": int(f[7]), "planned": int(f[9]),
                      "nstages": int(f[11]), "scale": float(f[13]), "walsh": int(f[15]), "marked": int(f[17]),
-                     "tail": int(f[19])}
+                     "tail": int(f[19]), "tma": int(f[21]), "dims": int(f[23]), "tok": int(f[25])}
     return res
 
 
@@ -61,3 +61,17 @@ def test_walsh_passes_are_planned(cases, name, hadamards, stages, tail):
     assert c["segment"] == 0 and c["walsh"] == 1 and c["planned"] == 1
     assert c["hb"] == hadamards and c["nstages"] == stages and c["marked"] == stages and c["tail"] == tail
     assert math.isclose(c["scale"], 0.5 ** (hadamards / 2), rel_tol=1e-15)
+
+
+def test_tensor_map_tiles(cases):
+    """complex64 passes whose index bits 0-3 are local load each tile by one
+    tensor-map copy when the copy's 128-byte swizzle costs the stages no more
+    bank conflicts than the searched swizzle: the box walks the local index in
+    order and that swizzle is the pass's shared-memory swizzle.  QFT-28's last
+    pass (stages on bits 4-6) keeps the per-thread copies."""
+    planned = [k for k, c in cases.items() if c["tma"]]
+    assert "qft28_first" in planned and "walsh_top" in planned and "sub_register" in planned
+    assert "qft28_last" not in planned and "walsh_low" not in planned
+    for k in planned:
+        assert cases[k]["tok"] == 1 and 2 <= cases[k]["dims"] <= 5, k
+    assert cases["qft28_first"]["dims"] == 4

@@ -24,6 +24,8 @@
 // transformed); a thread's copies sit at fixed offsets from the tile base.  Stage accesses use an XOR swizzle chosen per pass on the
 // host so that the lanes of each half-warp (quarter-warp for complex128) hit
 // distinct banks wherever the pass's bit layout allows it.
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -79,6 +81,15 @@ struct QftGeom {
 	uint64_t ntiles;
 	uint64_t istride;    // global element step between a thread's granules
 	double scale;
+	// Tiles by one tensor-map copy (complex64): the state as a tensor whose
+	// dimensions are runs of index bits, ascending -- local runs (split so
+	// that the innermost is 16 amplitudes = one 128-byte swizzle row and the
+	// others hold at most 256) are the box, outer runs are box-1 dimensions
+	// whose coordinates are the tile index bits of that run.
+	uint32_t tma, tma_dims;
+	uint32_t tma_outer[5], tma_shift[5], tma_len[5];
+	uint64_t tma_size[5], tma_stride[5];  // elements; bytes (dimension 0: the element)
+	uint32_t tma_box[5];
 	QftStage st[kQftMaxStages];
 	RootTable roots;
 };
@@ -125,7 +136,7 @@ __device__ __forceinline__ void stage_factors(uint64_t w, unsigned bhi, unsigned
 	}
 }
 
-__device__ __forceinline__ unsigned qft_phys(const QftGeom &g, unsigned j) {
+__host__ __device__ __forceinline__ unsigned qft_phys(const QftGeom &g, unsigned j) {
 	unsigned x = j;
 #pragma unroll
 	for(int k = 0; k < 3; ++k)
@@ -320,6 +331,43 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *b, unsigned parity) {
 	return ok != 0;
 }
 
+// Expect `bytes` of asynchronous copies on the barrier and arrive (the
+// barrier's count is 1 for tensor-map tiles: the issuing thread).
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *b, uint32_t bytes) {
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+
+// Tile o by one tensor-map copy: coordinates 0 on the box dimensions, the
+// tile index bits of each outer run on the others; completion on `bar`.
+__device__ __forceinline__ void tma_tile(void *dst, const CUtensorMap *tm, const QftGeom &g, uint64_t o, uint64_t *bar) {
+	int c[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+	for(unsigned i = 0; i < 5; ++i)
+		if(i < g.tma_dims && g.tma_outer[i]) c[i] = (int)((o >> g.tma_shift[i]) & ((1ull << g.tma_len[i]) - 1ull));
+	const uint32_t d = smem_u32(dst), m = smem_u32(bar);
+	const uint64_t t = reinterpret_cast<uint64_t>(tm);
+	switch(g.tma_dims) {
+		case 2:
+			asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+			             ::"r"(d), "l"(t), "r"(c[0]), "r"(c[1]), "r"(m) : "memory");
+			break;
+		case 3:
+			asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+			             ::"r"(d), "l"(t), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(m) : "memory");
+			break;
+		case 4:
+			asm volatile(
+				"cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+				::"r"(d), "l"(t), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(m) : "memory");
+			break;
+		default:
+			asm volatile(
+				"cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+				"[%7];" ::"r"(d), "l"(t), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(m) : "memory");
+			break;
+	}
+}
+
 // Upper bound on the polls of a tile's arrival (each poll may suspend the
 // thread for a while).  Past it the thread records the failure in the
 // handle's error word and goes on (every thread keeps the same barrier
@@ -401,15 +449,19 @@ __device__ __forceinline__ void qft_tail(const V *tile, V *dst, unsigned T, unsi
 // thread's first amplitude per stage [nstages][nthr], and one row of per-tile
 // factors per ring slot.  Everything is derived here from the geometry: the
 // launch needs no device program.
-template <typename R, int RB>
+template <typename R, int RB, bool TM>
 __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type), RB), 1)
-	k_qft_pass(typename Vec2<R>::type *a, const __grid_constant__ QftGeom g, int *err) {
+	k_qft_pass(typename Vec2<R>::type *a, const __grid_constant__ QftGeom g, const __grid_constant__ CUtensorMap tmap,
+	           int *err) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	constexpr unsigned per16 = 16 / sizeof(V);
 	constexpr unsigned kGranules = (1u << RB) / per16;  // 16-byte granules per thread per tile
 	const unsigned T = 1u << g.K, tid = threadIdx.x, nthr = blockDim.x;
-	V *ring = reinterpret_cast<V *>(smem_raw);
+	// TM (tiles by tensor-map copies): the ring starts on a 1024-byte
+	// boundary (the copy's 128-byte swizzle repeats every 1024 bytes of
+	// shared address).
+	V *ring = reinterpret_cast<V *>(TM ? smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u) : smem_raw);
 	V *ftab = ring + (size_t)g.slots * T;
 	V *orow = ftab + (size_t)g.nfrows * nthr;
 	QftStage *sst = reinterpret_cast<QftStage *>(orow + (size_t)g.slots * g.ot_stride);
@@ -418,7 +470,7 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 
 	if(tid < g.nstages) sst[tid] = g.st[tid];
 	if(tid == 0)
-		for(unsigned k = 0; k < g.slots; ++k) mbar_init(&mbar[k], nthr);
+		for(unsigned k = 0; k < g.slots; ++k) mbar_init(&mbar[k], TM ? 1u : nthr);
 	const uint64_t goff = qft_scatter(g, tid * per16);
 	const unsigned psm = qft_phys(g, tid * per16);
 	const unsigned gstep = nthr * per16;  // shared index step between a thread's granules
@@ -430,11 +482,22 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 	auto prefetch = [&](uint64_t o, unsigned slot) {
 		if(o < g.ntiles) {
 			const uint64_t base = qft_tile_base(g, o);
-			const V *src = a + base + goff;
-			V *dst = ring + (size_t)slot * T + psm;
+			if constexpr(TM) {
+				// One thread: the slot's earlier generic reads and writes are
+				// ordered before the copy by the barrier that precedes this call
+				// and the proxy fence.
+				if(tid == 0) {
+					asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+					mbar_arrive_expect_tx(&mbar[slot], (uint32_t)(T * sizeof(V)));
+					tma_tile(ring + (size_t)slot * T, &tmap, g, o, &mbar[slot]);
+				}
+			} else {
+				const V *src = a + base + goff;
+				V *dst = ring + (size_t)slot * T + psm;
 #pragma unroll
-			for(unsigned i = 0; i < kGranules; ++i) cp_async16(dst + i * gstep, src + i * g.istride);
-			cp_async_mbar_arrive(&mbar[slot]);
+				for(unsigned i = 0; i < kGranules; ++i) cp_async16(dst + i * gstep, src + i * g.istride);
+				cp_async_mbar_arrive(&mbar[slot]);
+			}
 			const unsigned st = tid >> 5;
 			if((tid & 31u) == 0 && st < g.nstages && sst[st].ot != kQftNone)
 				stage_factors<V>(base & sst[st].wmask & ~g.localmask, sst[st].bhi, sst[st].d,
@@ -464,13 +527,20 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 
 	const typename Scalar<V>::type s = (typename Scalar<V>::type)g.scale;
 	__syncthreads();  // tables and barrier initialisation visible
-	unsigned slot = 0, phase = 0;
+	unsigned slot = 0, phase = 0, stuck_phase = 0;
+	int stuck = -1;  // a slot whose tile did not arrive in time (its copy may still land)
 	for(; o < g.ntiles; o += gridDim.x) {
 		// The tile's copies (every thread's) are done once the slot's barrier
 		// completes this phase.
 		bool ready = false;
 		for(int it = 0; it < kQftWaitPolls && !ready; ++it) ready = mbar_try_wait(&mbar[slot], phase);
-		if(!ready) atomicExch(err, 1);
+		if(!ready) {
+			atomicExch(err, 1);
+			if constexpr(TM) {
+				stuck = (int)slot;
+				stuck_phase = phase;
+			}
+		}
 		V *tile = ring + (size_t)slot * T;
 		const V *ot = orow + slot * g.ot_stride;
 		const uint64_t tbase = qft_tile_base(g, o);
@@ -512,6 +582,13 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 		}
 	}
 	cp_async_wait_all();
+	// After a timeout, wait (bounded again) for the late copy before the
+	// shared memory is released.
+	if constexpr(TM) {
+		if(stuck >= 0)
+			for(int it = 0; it < kQftWaitPolls && !mbar_try_wait(&mbar[stuck], stuck_phase); ++it) {
+			}
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -602,7 +679,7 @@ struct Swizzle {
 
 // Plans the pass for storage values of vbytes bytes and RB register bits.
 bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r0, unsigned vbytes, unsigned RB,
-              QftGeom &g, bool walsh) {
+              QftGeom &g, bool walsh, bool allow_tma = false) {
 	const unsigned K = pass.K, n = pass.n, per16 = 16 / vbytes;
 	const unsigned lgran = RB - (per16 == 2 ? 1u : 0u);  // log2 of the granules per thread
 	if(K > 14 || K < RB + 5 || (1u << (K - RB)) > qft_max_threads(vbytes, (int)RB)) return false;
@@ -759,6 +836,49 @@ bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r
 					}
 				}
 	}
+	// Tensor-map tiles (complex64, when asked): the 128-byte swizzle the copy
+	// applies is shared index bits 1-3 ^= bits 4-6, so it is taken when it
+	// costs the stages no more bank conflicts than the searched swizzle.
+	g.tma = 0;
+	if(allow_tma && vbytes == 8 && K >= 4 && src_hi >= 6) {
+		Swizzle t;
+		for(int k = 0; k < 3; ++k) {
+			t.src[k] = 4u + (unsigned)k;
+			t.dst[k] = 1u + (unsigned)k;
+		}
+		bool fits = cost(t) <= best_cost;
+		for(unsigned l = 0; l < 4 && fits; ++l)
+			if(pass.lpos[l] != l) fits = false;  // the innermost run: index bits 0-3 at least
+		unsigned dims = 0, oshift = 0;
+		for(unsigned b = 0; b < n && fits;) {
+			const bool local = (g.localmask >> b) & 1ull;
+			unsigned e = b;
+			while(e < n && (((g.localmask >> e) & 1ull) != 0) == local) ++e;
+			for(unsigned p0 = b; p0 < e && fits;) {
+				// Local runs in pieces: bits 0-3, then up to 8 bits; an outer run whole.
+				const unsigned len = !local ? e - p0 : (p0 == 0 ? 4u : std::min(8u, e - p0));
+				if(dims == 5 || len > 32 || ((1ull << p0) * vbytes) >= (1ull << 40)) {
+					fits = false;
+					break;
+				}
+				g.tma_outer[dims] = local ? 0u : 1u;
+				g.tma_shift[dims] = local ? 0u : oshift;
+				g.tma_len[dims] = len;
+				g.tma_size[dims] = 1ull << len;
+				g.tma_stride[dims] = (1ull << p0) * vbytes;
+				g.tma_box[dims] = local ? (1u << len) : 1u;
+				if(!local) oshift += len;
+				++dims;
+				p0 += len;
+			}
+			b = e;
+		}
+		if(fits) {
+			g.tma = 1;
+			g.tma_dims = dims;
+			best = t;
+		}
+	}
 	for(int k = 0; k < 3; ++k) {
 		g.sw_src[k] = best.src[k];
 		g.sw_dst[k] = best.dst[k];
@@ -791,17 +911,54 @@ bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r
 	return true;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links the runtime only).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn tile_map_encoder() {
+	static EncodeTiledFn fn = [] {
+		void *p = nullptr;
+		cudaDriverEntryPointQueryResult q{};
+		if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+		   q != cudaDriverEntryPointSuccess) {
+			cudaGetLastError();
+			return (EncodeTiledFn) nullptr;
+		}
+		return reinterpret_cast<EncodeTiledFn>(p);
+	}();
+	return fn;
+}
+
+// The state (8-byte amplitudes) as the pass's tensor, 128-byte swizzle.
+bool encode_tile_map(CUtensorMap &m, void *a, const QftGeom &g) {
+	const EncodeTiledFn enc = tile_map_encoder();
+	if(!enc) return false;
+	cuuint64_t size[5], stride[4];
+	cuuint32_t box[5], estr[5];
+	for(unsigned i = 0; i < g.tma_dims; ++i) {
+		size[i] = g.tma_size[i];
+		box[i] = g.tma_box[i];
+		estr[i] = 1;
+		if(i) stride[i - 1] = g.tma_stride[i];
+	}
+	return enc(&m, CU_TENSOR_MAP_DATA_TYPE_UINT64, g.tma_dims, a, size, stride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+	           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+	       CUDA_SUCCESS;
+}
+
 template <typename R, int RB>
 bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r0,
              bool walsh) {
 	typedef typename Vec2<R>::type V;
 	QftGeom g;
-	if(!c.err || !plan_qft(pass, hb, r0, (unsigned)sizeof(V), (unsigned)RB, g, walsh)) return false;
+	if(!c.err || !plan_qft(pass, hb, r0, (unsigned)sizeof(V), (unsigned)RB, g, walsh, true)) return false;
 	const unsigned nthr = 1u << (g.K - RB);
 	const size_t T = size_t(1) << g.K;
 	auto smem_for = [&](unsigned slots) {
 		return (slots * T + (size_t)g.nfrows * nthr + (size_t)slots * g.ot_stride) * sizeof(V) +
-		       kQftMaxStages * sizeof(QftStage) + slots * 8 + (size_t)g.nstages * nthr * 2;
+		       kQftMaxStages * sizeof(QftStage) + slots * 8 + (size_t)g.nstages * nthr * 2 + (g.tma ? 1024 : 0);
 	};
 	int dev = 0, max_optin = 0;
 	check_cuda(cudaGetDevice(&dev), "qft device");
@@ -809,9 +966,13 @@ bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass, const std::vect
 	g.slots = smem_for(3) <= (size_t)max_optin ? 3u : 2u;
 	const size_t smem = smem_for(g.slots);
 	if(smem > (size_t)max_optin) return false;
-	check_cuda(cudaFuncSetAttribute(k_qft_pass<R, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "qft smem");
+	CUtensorMap tmap;
+	std::memset(&tmap, 0, sizeof(tmap));
+	if(g.tma && !encode_tile_map(tmap, a, g)) g.tma = 0;  // no encoder: per-thread copies (same swizzle)
+	auto kern = g.tma ? k_qft_pass<R, RB, true> : k_qft_pass<R, RB, false>;
+	check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "qft smem");
 	const uint64_t grid = std::min<uint64_t>(g.ntiles, (uint64_t)c.num_sms);
-	k_qft_pass<R, RB><<<(unsigned)grid, nthr, smem, c.stream>>>(static_cast<V *>(a), g, c.err);
+	kern<<<(unsigned)grid, nthr, smem, c.stream>>>(static_cast<V *>(a), g, tmap, c.err);
 	check_cuda(cudaGetLastError(), "qft pass");
 	if(c.launches) ++*c.launches;
 	return true;
