@@ -79,6 +79,17 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
 	for(int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Sixteen TMEM columns of this thread's lane, without waiting (the caller
+// waits once for a batch of these with tmem_wait_ld).
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&r)[16]) {
+	asm volatile(
+		"tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+		: "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+		  "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+		: "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 struct TcGateGeom {
 	unsigned n, k;
 	unsigned tpos_sorted[8];  // target bit positions, ascending (for the group base)
@@ -189,15 +200,18 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gate(float2 *a, TcGateGeom g,
 		asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 		if(ok) {
 			// Row tid of D: columns c (real part) and D + c (imaginary part).
+			// All 2D columns in flight together, one wait.
 			const uint32_t lane_addr = tbase + ((32u * warp) << 16);
+			uint32_t re[D / 16][16], im[D / 16][16];
 #pragma unroll
-			for(int c0 = 0; c0 < D; c0 += 8) {
-				float re[8], im[8];
-				tmem_ld8(lane_addr + c0, re);
-				tmem_ld8(lane_addr + D + c0, im);
-#pragma unroll
-				for(int i = 0; i < 8; ++i) a[gb + soff[c0 + i]] = make_float2(re[i], im[i]);
+			for(int q = 0; q < D / 16; ++q) {
+				tmem_ld16_nowait(lane_addr + 16 * q, re[q]);
+				tmem_ld16_nowait(lane_addr + D + 16 * q, im[q]);
 			}
+			tmem_wait_ld();
+#pragma unroll
+			for(int c = 0; c < D; ++c)
+				a[gb + soff[c]] = make_float2(__uint_as_float(re[c / 16][c % 16]), __uint_as_float(im[c / 16][c % 16]));
 		}
 		asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 		__syncthreads();
