@@ -61,21 +61,23 @@ static FusedPass make(unsigned n, const std::vector<unsigned> &local, const std:
 // A QFT segment, else a Walsh segment (Hadamards only), as launch_qft_pass
 // tries them; for a Walsh plan, every stage is marked and the tail (if any)
 // sits on the lowest bits.
-static void check(const char *name, const FusedPass &p) {
+static void check(const char *name, const FusedPass &p, unsigned vb = 8) {
 	std::vector<unsigned> hb;
 	unsigned r0 = 0;
 	const bool seg = qft_segment(p, hb, r0);
 	bool walsh = false;
+	WalshDiag dg;
 	if(!seg) {
-		walsh = walsh_segment(p, hb);
+		walsh = walsh_segment(p, hb, dg);
 		r0 = p.n;
 	}
 	int planned = -1;
-	unsigned nstages = 0, marked = 0, tail = 0, tma = 0, tdims = 0, tok = 1;
+	unsigned nstages = 0, marked = 0, tail = 0, tma = 0, tdims = 0, tok = 1, dside = 0;
 	double scale = 0.0;
 	if(seg || walsh) {
 		QftGeom g{};
-		planned = plan_qft(p, hb, r0, 8, 5, g, walsh, true) ? 1 : 0;
+		planned = plan_qft(p, hb, r0, vb, vb == 8 ? 5 : 4, g, walsh, true, &dg) ? 1 : 0;
+		dside = g.dside;
 		nstages = g.nstages;
 		scale = g.scale;
 		for(unsigned s = 0; s < g.nstages; ++s) {
@@ -92,7 +94,7 @@ static void check(const char *name, const FusedPass &p) {
 			uint64_t elems = 1;
 			unsigned bit = 0, local = 0;
 			for(unsigned i = 0; i < g.tma_dims; ++i) {
-				if(g.tma_stride[i] != (8ull << bit) && i) tok = 0;
+				if(g.tma_stride[i] != ((uint64_t)vb << bit) && i) tok = 0;
 				if(!g.tma_outer[i]) {
 					elems *= g.tma_box[i];
 					for(unsigned b = 0; b < g.tma_len[i]; ++b)
@@ -102,15 +104,16 @@ static void check(const char *name, const FusedPass &p) {
 				}
 				bit += g.tma_len[i];
 			}
-			if(elems != (1ull << g.K) || bit != p.n || g.tma_box[0] * 8 != 128) tok = 0;
+			if(elems != (uint64_t(vb / 8) << g.K) || bit != p.n || g.tma_box[0] * 8 != 128) tok = 0;
 			for(unsigned j = 0; j < (1u << g.K); ++j) {
-				const unsigned byte = j * 8, tswz = byte ^ (((byte >> 7) & 7u) << 4);
-				if(tswz != qft_phys(g, j) * 8) tok = 0;
+				const unsigned byte = j * vb, tswz = byte ^ (((byte >> 7) & 7u) << 4);
+				if(tswz != qft_phys(g, j) * vb) tok = 0;
 			}
 		}
 	}
-	std::printf("case %s segment %d hb %zu r0 %u planned %d nstages %u scale %.17g walsh %d marked %u tail %u tma %u dims %u tok %u\n",
-	            name, (int)seg, hb.size(), seg ? r0 : 0u, planned, nstages, scale, (int)walsh, marked, tail, tma, tdims, tok);
+	std::printf(
+		"case %s segment %d hb %zu r0 %u planned %d nstages %u scale %.17g walsh %d marked %u tail %u tma %u dims %u tok %u dside %u\n",
+		name, (int)seg, hb.size(), seg ? r0 : 0u, planned, nstages, scale, (int)walsh, marked, tail, tma, tdims, tok, dside);
 }
 
 static std::vector<unsigned> range(unsigned lo, unsigned hi) {  // [lo, hi)
@@ -143,5 +146,37 @@ int main() {
 	check("walsh_top", make(24, wl, down(23, 16), 0, false, false, true));
 	check("walsh_low", make(24, range(0, 13), down(12, 0), 0, false, false, true));
 	check("walsh_scattered", make(24, range(0, 13), {3, 11, 7, 9}, 0, false, false, true));
+	// Hadamards on bits 7..0 with a ring of controlled phases after them (the
+	// layered circuits' last pass of a layer), before them, on both sides
+	// (not a segment), and with a phase flip.
+	auto ring = [&](FusedPass q, bool before, bool after, bool flip) {
+		std::vector<FusedOp> cps;
+		for(unsigned b = 0; b < 24; ++b) {
+			FusedOp f{};
+			f.kind = kFCP;
+			f.mask = (1ull << b) | (1ull << ((b + 1) % 24));
+			f.cr = std::cos(0.1 * b);
+			f.ci = std::sin(0.1 * b);
+			cps.push_back(f);
+		}
+		if(flip) {
+			FusedOp f{};
+			f.kind = kFFlip;
+			f.state = 12345;
+			cps.push_back(f);
+		}
+		if(before) q.ops.insert(q.ops.begin(), cps.begin(), cps.end());
+		if(after) q.ops.insert(q.ops.end(), cps.begin(), cps.end());
+		return q;
+	};
+	check("walsh_diag_after", ring(make(24, range(0, 13), down(7, 0), 0, false, false, true), false, true, false));
+	check("walsh_diag_before", ring(make(24, range(0, 13), down(7, 0), 0, false, false, true), true, false, true));
+	check("walsh_diag_both", ring(make(24, range(0, 13), down(7, 0), 0, false, false, true), true, true, false));
+	check("walsh_diag_after_top", ring(make(24, wl, down(23, 16), 0, false, false, true), false, true, false));
+	// complex128 (12-bit tiles): bits {0..3} and the pass's 8 Hadamard bits.
+	std::vector<unsigned> c128 = range(0, 4), c128t = range(20, 28);
+	c128.insert(c128.end(), c128t.begin(), c128t.end());
+	check("qft28_first_c128", make(28, c128, down(27, 20), 0), 16);
+	check("qft28_last_c128", make(28, range(0, 12), down(11, 0), 0), 16);
 	return 0;
 }

@@ -54,7 +54,7 @@ def run_gpu(n, amps, ops, prec, qft_pass=True, fused_qubits=0):
 
 def oracle(n, amps, ops):
     r = O.OracleRegister(n, amps=amps)
-    r.run([O.Op(kind=o.kind, q0=o.q0, q1=o.q1, theta=o.theta) for o in ops])
+    r.run([O.Op(kind=o.kind, q0=o.q0, q1=o.q1, theta=o.theta, state=o.state) for o in ops])
     return r.amplitudes()
 
 
@@ -191,3 +191,23 @@ def test_qft_pass_large_against_exact(prec):
     got, st = run_gpu(n, amps, tq.qft_ops(n), prec)
     assert st["qft_passes"] >= 2
     assert O.rel_l2(want, got) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", [tq.FP64, tq.FP32])
+@pytest.mark.parametrize("side", ["after", "before"])
+def test_walsh_pass_with_ring_phases(prec, side):
+    """Hadamards on the lowest qubits' bits 7..0 of a 20-qubit state with a
+    ring of controlled phases and a phase flip after them (applied in the
+    fused tail) or before them (applied to each arriving tile), as the layered
+    circuits' last pass of a layer and its inverse; against the oracle.
+    complex128's 4-bit stages leave 4 Hadamards for the last stage, more than
+    the fused tail takes: its pass with the phases after runs as a radix pass."""
+    n = 20
+    rng = np.random.default_rng(5 if side == "after" else 6)
+    th = rng.uniform(0, 2 * np.pi, n)
+    hs = [tq.h(q) for q in range(n - 8, n)]
+    diag = [tq.cphase(q, (q + 1) % n, float(th[q])) for q in range(n)] + [tq.phase_flip(12345)]
+    ops = hs + diag if side == "after" else diag + hs
+    a = rng.standard_normal(2 << n)
+    a /= np.linalg.norm(a)
+    check(n, a, ops, prec, expect_qft=not (prec == tq.FP64 and side == "after"))

@@ -19,6 +19,7 @@ def cases(tmp_path_factory):
         pytest.skip("nvcc not available")
     exe = str(tmp_path_factory.mktemp("qft") / "qft_plan_check")
     subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=compute_100a", "-std=c++17", "--expt-relaxed-constexpr",
+                    "-DTMFQS_QFT_PLAN_ONLY",
                     "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "tmfqsfullstate_b200", "csrc"),
                     "-o", exe, os.path.join(ROOT, "tests", "qft_plan_check.cu")], check=True, timeout=600)
     out = subprocess.run([exe], capture_output=True, text=True, check=True, timeout=60).stdout
@@ -27,7 +28,7 @@ def cases(tmp_path_factory):
         f = line.split()
         res[f[1]] = {"segment": int(f[3]), "hb": int(f[5]), "r0": int(f[7]), "planned": int(f[9]),
                      "nstages": int(f[11]), "scale": float(f[13]), "walsh": int(f[15]), "marked": int(f[17]),
-                     "tail": int(f[19]), "tma": int(f[21]), "dims": int(f[23]), "tok": int(f[25])}
+                     "tail": int(f[19]), "tma": int(f[21]), "dims": int(f[23]), "tok": int(f[25]), "dside": int(f[27])}
     return res
 
 
@@ -75,3 +76,17 @@ def test_tensor_map_tiles(cases):
     for k in planned:
         assert cases[k]["tok"] == 1 and 2 <= cases[k]["dims"] <= 5, k
     assert cases["qft28_first"]["dims"] == 4
+    # complex128: 8-amplitude rows
+    assert cases["qft28_first_c128"]["planned"] == 1 and cases["qft28_last_c128"]["planned"] == 1
+
+
+def test_walsh_with_diagonal_ops(cases):
+    """Hadamards with controlled phases (and flips) all after them run the
+    phases in the fused tail, all before them on each arriving tile; on both
+    sides they are no segment, and after them without a fused tail (the
+    Hadamards on the top bits) the pass goes to the radix kernel."""
+    after, before = cases["walsh_diag_after"], cases["walsh_diag_before"]
+    assert after["walsh"] == 1 and after["planned"] == 1 and after["dside"] == 2 and after["tail"] == 1
+    assert before["walsh"] == 1 and before["planned"] == 1 and before["dside"] == 1
+    assert cases["walsh_diag_both"]["walsh"] == 0
+    assert cases["walsh_diag_after_top"]["walsh"] == 1 and cases["walsh_diag_after_top"]["planned"] == 0
