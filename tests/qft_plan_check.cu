@@ -66,18 +66,16 @@ static void check(const char *name, const FusedPass &p, unsigned vb = 8) {
 	unsigned r0 = 0;
 	const bool seg = qft_segment(p, hb, r0);
 	bool walsh = false;
-	WalshDiag dg;
 	if(!seg) {
-		walsh = walsh_segment(p, hb, dg);
+		walsh = walsh_segment(p, hb);
 		r0 = p.n;
 	}
 	int planned = -1;
-	unsigned nstages = 0, marked = 0, tail = 0, tma = 0, tdims = 0, tok = 1, dside = 0;
+	unsigned nstages = 0, marked = 0, tail = 0, tma = 0, tdims = 0, tok = 1;
 	double scale = 0.0;
 	if(seg || walsh) {
 		QftGeom g{};
-		planned = plan_qft(p, hb, r0, vb, vb == 8 ? 5 : 4, g, walsh, true, &dg) ? 1 : 0;
-		dside = g.dside;
+		planned = plan_qft(p, hb, r0, vb, vb == 8 ? 5 : 4, g, walsh, true) ? 1 : 0;
 		nstages = g.nstages;
 		scale = g.scale;
 		for(unsigned s = 0; s < g.nstages; ++s) {
@@ -111,9 +109,8 @@ static void check(const char *name, const FusedPass &p, unsigned vb = 8) {
 			}
 		}
 	}
-	std::printf(
-		"case %s segment %d hb %zu r0 %u planned %d nstages %u scale %.17g walsh %d marked %u tail %u tma %u dims %u tok %u dside %u\n",
-		name, (int)seg, hb.size(), seg ? r0 : 0u, planned, nstages, scale, (int)walsh, marked, tail, tma, tdims, tok, dside);
+	std::printf("case %s segment %d hb %zu r0 %u planned %d nstages %u scale %.17g walsh %d marked %u tail %u tma %u dims %u tok %u\n",
+	            name, (int)seg, hb.size(), seg ? r0 : 0u, planned, nstages, scale, (int)walsh, marked, tail, tma, tdims, tok);
 }
 
 static std::vector<unsigned> range(unsigned lo, unsigned hi) {  // [lo, hi)
@@ -147,8 +144,8 @@ int main() {
 	check("walsh_low", make(24, range(0, 13), down(12, 0), 0, false, false, true));
 	check("walsh_scattered", make(24, range(0, 13), {3, 11, 7, 9}, 0, false, false, true));
 	// Hadamards on bits 7..0 with a ring of controlled phases after them (the
-	// layered circuits' last pass of a layer), before them, on both sides
-	// (not a segment), and with a phase flip.
+	// layered circuits' last pass of a layer), before them, on both sides, and
+	// with a phase flip: no Walsh segment (the radix pass takes them).
 	auto ring = [&](FusedPass q, bool before, bool after, bool flip) {
 		std::vector<FusedOp> cps;
 		for(unsigned b = 0; b < 24; ++b) {

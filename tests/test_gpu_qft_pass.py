@@ -195,13 +195,11 @@ def test_qft_pass_large_against_exact(prec):
 
 @pytest.mark.parametrize("prec", [tq.FP64, tq.FP32])
 @pytest.mark.parametrize("side", ["after", "before"])
-def test_walsh_pass_with_ring_phases(prec, side):
-    """Hadamards on the lowest qubits' bits 7..0 of a 20-qubit state with a
-    ring of controlled phases and a phase flip after them (applied in the
-    fused tail) or before them (applied to each arriving tile), as the layered
-    circuits' last pass of a layer and its inverse; against the oracle.
-    complex128's 4-bit stages leave 4 Hadamards for the last stage, more than
-    the fused tail takes: its pass with the phases after runs as a radix pass."""
+def test_walsh_with_ring_phases_stays_radix(prec, side):
+    """Hadamards on bits 7..0 of a 20-qubit state with a ring of controlled
+    phases and a phase flip after or before them (the layered circuits' last
+    pass of a layer and its inverse) are no Walsh segment: the radix pass runs
+    them; against the oracle."""
     n = 20
     rng = np.random.default_rng(5 if side == "after" else 6)
     th = rng.uniform(0, 2 * np.pi, n)
@@ -210,4 +208,4 @@ def test_walsh_pass_with_ring_phases(prec, side):
     ops = hs + diag if side == "after" else diag + hs
     a = rng.standard_normal(2 << n)
     a /= np.linalg.norm(a)
-    check(n, a, ops, prec, expect_qft=not (prec == tq.FP64 and side == "after"))
+    check(n, a, ops, prec, expect_qft=False)

@@ -492,12 +492,12 @@ struct Planner {
 			++npass;
 			PassTimer timer(h, TMFQS_KT_FUSED, sweep_bytes(h));
 			const bool qft = twiddle && h->opt_radix && h->opt_qft_pass &&
-			                 tqb::launch_qft_pass(ctx(h), h->precision, h->amps, pass, true, mirror);
+			                 tqb::launch_qft_pass(ctx(h), h->precision, h->amps, pass, mirror == nullptr);
 			if(qft) ++h->stats.qft_passes;
 			const bool done = qft || (twiddle && h->opt_radix &&
 			                          tqb::launch_radix_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes,
 			                                                 mirror));
-			mirrored = done && mirror;
+			mirrored = !qft && done && mirror;
 			if(!done) tqb::launch_fused_pass(ctx(h), h->precision, h->amps, pass, h->dev_prog, h->dev_prog_bytes);
 			++h->stats.fused_passes;
 		}

@@ -185,12 +185,8 @@ bool launch_radix_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &p
 // c of the register) in the fast forms.  Returns false (nothing launched) when
 // the pass is not such a segment or its layout does not qualify.
 // A QFT segment pass (k_qft_pass); with allow_walsh also a pass of Hadamards
-// (with controlled phases and phase flips all before or all after them).
-// With `mirror`, the result is also written there (only passes whose last
-// stage is fused into the copy-out do).  False: not such a pass, or it does
-// not fit the kernel's tiles.
-bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, bool allow_walsh,
-                     void *mirror = nullptr);
+// only.  False: the pass is neither (or does not fit the kernel's tiles).
+bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, bool allow_walsh);
 
 // ---------------------------------------------------------------------------
 // Adjoint gradient (adjoint.cu)

@@ -41,7 +41,6 @@ namespace {
 
 constexpr unsigned kQftMaxStages = 4;
 constexpr unsigned kQftMaxRuns = 8;
-constexpr unsigned kQftMaxDiag = 32;  // diagonal ops of a Walsh segment
 
 // Threads per CTA: 2^(K - RB) for tiles of 2^K amplitudes, at most 512 (a
 // complex64 kernel with 4 register bits), else 256.
@@ -91,15 +90,6 @@ struct QftGeom {
 	uint32_t tma_outer[5], tma_shift[5], tma_len[5];
 	uint64_t tma_size[5], tma_stride[5];  // elements; bytes (dimension 0: the element)
 	uint32_t tma_box[5];
-	// Diagonal ops of a Walsh segment (controlled phases and phase flips; they
-	// commute): before its Hadamards (dside 1, applied to each arriving tile)
-	// or after them (dside 2, applied in the fused tail).  Entry k acts on basis
-	// state x when x contains dmask[k] (a flip: when x equals dmask[k]); per
-	// index byte a table of 32-bit entry sets, per group of 8 entries a table
-	// of phase products, both built by each CTA in shared memory.
-	uint32_t dside, dcount, dbytes, dgroups, dflip;
-	uint64_t dmask[kQftMaxDiag];
-	double dcr[kQftMaxDiag], dci[kQftMaxDiag];
 	QftStage st[kQftMaxStages];
 	RootTable roots;
 };
@@ -228,50 +218,9 @@ __device__ __forceinline__ void walsh_ladder(V (&v)[1 << RB]) {
 	}
 }
 
-// The diagonal factor of a Walsh segment's phases and flips for basis state
-// x: the set of entries acting on x is the AND of one table word per index
-// byte; their phase product, one table per 8 entries.
-template <typename V>
-struct DiagCtx {
-	const uint32_t *tab;  // [bytes][256] entry sets
-	const V *q;           // [groups][256] phase products (FP64, rounded once)
-	unsigned nbytes, ngroups;
-};
-
-// Entry set of the index bytes of x outside `vary` (a bit per byte), and of
-// those in it; at most 5 index bytes (40 qubits).
-template <typename V>
-__device__ __forceinline__ uint32_t diag_hits(const DiagCtx<V> &d, uint64_t x, unsigned vary, bool inside) {
-	uint32_t hit = ~0u;
-#pragma unroll
-	for(unsigned j = 0; j < 5; ++j)
-		if(j < d.nbytes && (((vary >> j) & 1u) != 0) == inside) hit &= d.tab[(j << 8) | ((unsigned)(x >> (8 * j)) & 255u)];
-	return hit;
-}
-
-// The phase product of an entry set (at most 4 groups of 8 entries).
-template <typename V>
-__device__ __forceinline__ V diag_phase(const DiagCtx<V> &d, uint32_t hit) {
-	V f = d.q[hit & 255u];
-#pragma unroll
-	for(unsigned k = 1; k < 4; ++k)
-		if(k < d.ngroups) f = vmul(f, d.q[(k << 8) | ((hit >> (8 * k)) & 255u)]);
-	return f;
-}
-
-// Bytes of a 64-bit offset mask that hold set bits (bit j: byte j).
-__device__ __forceinline__ unsigned bytes_of(uint64_t m) {
-	unsigned b = 0;
-#pragma unroll
-	for(unsigned j = 0; j < 5; ++j)
-		if((m >> (8 * j)) & 255ull) b |= 1u << j;
-	return b;
-}
-
 template <typename V, int RB, int D, bool TW, bool SC, bool TOP, bool W = false>
 __device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
-                                              const V *ot, typename Scalar<V>::type s, const RootTable &roots, V *gdst,
-                                              const DiagCtx<V> *dc = nullptr) {
+                                              const V *ot, typename Scalar<V>::type s, const RootTable &roots, V *gdst) {
 	// TOP: the register bits are the tile's top local bits in order, so the
 	// offsets are compile-time constants added to the thread's base.
 	constexpr int kTop = qft_tile_bits(sizeof(V));
@@ -287,11 +236,8 @@ __device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsign
 			if((r >> i) & 1) x ^= roff[i];
 		v[r] = TOP ? tile[pbase + x] : tile[x];
 	}
-	if constexpr(W) {
-		walsh_ladder<V, RB, D>(v);
-	} else {
-		qft_stage<V, RB, D>(v, roots);
-	}
+	if constexpr(W) walsh_ladder<V, RB, D>(v);
+	else qft_stage<V, RB, D>(v, roots);
 	if constexpr(TW) {
 		V f[D];
 #pragma unroll
@@ -334,12 +280,11 @@ __device__ __forceinline__ void qft_stage_run(V *tile, const QftStage &S, unsign
 
 template <typename V, int RB, int D>
 __device__ __forceinline__ void qft_stage_flags(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
-                                                const V *ot, typename Scalar<V>::type s, const RootTable &roots, V *gdst,
-                                                const DiagCtx<V> *dc) {
+                                                const V *ot, typename Scalar<V>::type s, const RootTable &roots, V *gdst) {
 	const bool tw = S.fl != kQftNone;
 	if(S.walsh) {
-		if(S.scaled) qft_stage_run<V, RB, D, false, true, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, gdst, dc);
-		else qft_stage_run<V, RB, D, false, false, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr, dc);
+		if(S.scaled) qft_stage_run<V, RB, D, false, true, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, gdst);
+		else qft_stage_run<V, RB, D, false, false, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
 	} else if(tw) {
 		if(S.scaled) qft_stage_run<V, RB, D, true, true, false>(tile, S, pbase, frow, nthr, ot, s, roots, gdst);
 		else if(S.top) qft_stage_run<V, RB, D, true, false, true>(tile, S, pbase, frow, nthr, ot, s, roots, nullptr);
@@ -353,13 +298,13 @@ __device__ __forceinline__ void qft_stage_flags(V *tile, const QftStage &S, unsi
 template <typename V, int RB>
 __device__ __forceinline__ void qft_stage_dispatch(V *tile, const QftStage &S, unsigned pbase, const V *frow, unsigned nthr,
                                                    const V *ot, typename Scalar<V>::type s, const RootTable &roots,
-                                                   V *gdst, const DiagCtx<V> *dc) {
+                                                   V *gdst) {
 	switch(S.d) {
-		case 1: qft_stage_flags<V, RB, 1>(tile, S, pbase, frow, nthr, ot, s, roots, gdst, dc); break;
-		case 2: qft_stage_flags<V, RB, 2>(tile, S, pbase, frow, nthr, ot, s, roots, gdst, dc); break;
-		case 3: qft_stage_flags<V, RB, 3>(tile, S, pbase, frow, nthr, ot, s, roots, gdst, dc); break;
-		case 4: qft_stage_flags<V, RB, 4>(tile, S, pbase, frow, nthr, ot, s, roots, gdst, dc); break;
-		case 5: if constexpr(RB >= 5) qft_stage_flags<V, RB, 5>(tile, S, pbase, frow, nthr, ot, s, roots, gdst, dc); break;
+		case 1: qft_stage_flags<V, RB, 1>(tile, S, pbase, frow, nthr, ot, s, roots, gdst); break;
+		case 2: qft_stage_flags<V, RB, 2>(tile, S, pbase, frow, nthr, ot, s, roots, gdst); break;
+		case 3: qft_stage_flags<V, RB, 3>(tile, S, pbase, frow, nthr, ot, s, roots, gdst); break;
+		case 4: qft_stage_flags<V, RB, 4>(tile, S, pbase, frow, nthr, ot, s, roots, gdst); break;
+		case 5: if constexpr(RB >= 5) qft_stage_flags<V, RB, 5>(tile, S, pbase, frow, nthr, ot, s, roots, gdst); break;
 		default: break;
 	}
 }
@@ -445,7 +390,7 @@ __host__ __device__ constexpr int brev_bits(int r, int d) {
 // D-1-i, so register r holds element brev(r).
 template <typename V, int D, bool W>
 __device__ __forceinline__ void qft_tail(const V *tile, V *dst, unsigned T, unsigned tid, unsigned nthr, const QftGeom &g,
-                                         typename Scalar<V>::type s, const DiagCtx<V> *dc, uint64_t xtile, V *mdst) {
+                                         typename Scalar<V>::type s) {
 	constexpr unsigned E = 1u << D;
 	unsigned pe[E];
 #pragma unroll
@@ -473,16 +418,8 @@ __device__ __forceinline__ void qft_tail(const V *tile, V *dst, unsigned T, unsi
 		V out[E];
 #pragma unroll
 		for(int r = 0; r < (int)E; ++r) out[brev_bits(r, D)] = vscale(v[r], s);
-		if(dc) {
-			// Phases and flips after the Hadamards, on the outputs (the group's
-			// 2^D consecutive amplitudes differ in byte 0 only).
-			const uint32_t hc = diag_hits(*dc, xtile + j, 1u, false);
-#pragma unroll
-			for(unsigned e = 0; e < E; ++e) out[e] = vmul(out[e], diag_phase(*dc, hc & diag_hits(*dc, xtile + j + e, 1u, true)));
-		}
 		// 32-byte stores where a group spans whole sectors (sm_100 vector
-		// width): a lane then writes full sectors, not halves.  The optional
-		// second destination is a checkpoint copy of the result.
+		// width): a lane then writes full sectors, not halves.
 		auto store = [&](V *d) {
 			if constexpr(sizeof(V) == 8 && E >= 4) {
 #pragma unroll
@@ -507,7 +444,6 @@ __device__ __forceinline__ void qft_tail(const V *tile, V *dst, unsigned T, unsi
 			}
 		};
 		store(dst);
-		if(mdst) store(mdst);
 	}
 }
 
@@ -516,10 +452,10 @@ __device__ __forceinline__ void qft_tail(const V *tile, V *dst, unsigned T, unsi
 // thread's first amplitude per stage [nstages][nthr], and one row of per-tile
 // factors per ring slot.  Everything is derived here from the geometry: the
 // launch needs no device program.
-template <typename R, int RB, bool TM, bool DG>
+template <typename R, int RB, bool TM>
 __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type), RB), 1)
 	k_qft_pass(typename Vec2<R>::type *a, const __grid_constant__ QftGeom g, const __grid_constant__ CUtensorMap tmap,
-	           typename Vec2<R>::type *mirror, int *err) {
+	           int *err) {
 	typedef typename Vec2<R>::type V;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	constexpr unsigned per16 = 16 / sizeof(V);
@@ -534,34 +470,6 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 	QftStage *sst = reinterpret_cast<QftStage *>(orow + (size_t)g.slots * g.ot_stride);
 	uint64_t *mbar = reinterpret_cast<uint64_t *>(sst + kQftMaxStages);  // [slots]: arrival of each slot's tile
 	uint16_t *spst = reinterpret_cast<uint16_t *>(mbar + g.slots);
-	// A Walsh segment's diagonal tables: [bytes][256] entry sets, [groups][256] phase products.
-	uint32_t *dtab = reinterpret_cast<uint32_t *>(
-		(reinterpret_cast<uintptr_t>(spst + (size_t)g.nstages * nthr) + 15) & ~uintptr_t(15));
-	V *dq = reinterpret_cast<V *>(dtab + (size_t)g.dbytes * 256);
-	if constexpr(DG) {
-		for(unsigned e = tid; e < g.dbytes * 256; e += nthr) {
-			const unsigned j = e >> 8, v = e & 255u;
-			uint32_t bits = 0;
-			for(unsigned k = 0; k < g.dcount; ++k) {
-				const unsigned mb = (unsigned)(g.dmask[k] >> (8 * j)) & 255u;
-				const bool on = ((g.dflip >> k) & 1u) ? v == mb : (v & mb) == mb;
-				bits |= (on ? 1u : 0u) << k;
-			}
-			dtab[e] = bits;
-		}
-		for(unsigned e = tid; e < g.dgroups * 256; e += nthr) {
-			const unsigned grp = e >> 8, v = e & 255u;
-			double pr = 1.0, pi = 0.0;
-			for(unsigned b = 0; b < 8; ++b) {
-				const unsigned k = 8 * grp + b;
-				if(k >= g.dcount || !((v >> b) & 1u)) continue;
-				const double tr = pr * g.dcr[k] - pi * g.dci[k];
-				pi = pr * g.dci[k] + pi * g.dcr[k];
-				pr = tr;
-			}
-			dq[e] = to_storage<V>(pr, pi);
-		}
-	}
 
 	if(tid < g.nstages) sst[tid] = g.st[tid];
 	if(tid == 0)
@@ -616,7 +524,6 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 		if(S.fl != kQftNone) stage_factors<V>(qft_scatter(g, jt) & S.wmask, S.bhi, S.d, ftab + (size_t)S.fl * nthr + tid, nthr);
 		if(st + 1 == g.nstages) slast = qft_scatter(g, jt);
 	}
-	const DiagCtx<V> dctx{dtab, dq, g.dbytes, g.dgroups};
 	const bool direct = sst[g.nstages - 1].direct != 0;
 	const bool tail = sst[g.nstages - 1].tail != 0, wtail = sst[g.nstages - 1].walsh != 0;
 	const unsigned nrun = tail ? g.nstages - 1 : g.nstages;  // stages run through shared memory
@@ -640,30 +547,12 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 		V *tile = ring + (size_t)slot * T;
 		const V *ot = orow + slot * g.ot_stride;
 		const uint64_t tbase = qft_tile_base(g, o);
-		if constexpr(DG) {
-			if(g.dside == 1) {
-				// Phases and flips before the Hadamards: each thread scales the
-				// granules it would copy (the index bytes its granules share are
-				// looked up once), then the stages read the scaled tile.
-				const uint64_t x0 = tbase | goff;
-				const unsigned vary = bytes_of((uint64_t)(kGranules - 1) * g.istride | (per16 - 1));
-				const uint32_t hc = diag_hits(dctx, x0, vary, false);
-#pragma unroll
-				for(unsigned i = 0; i < kGranules; ++i)
-#pragma unroll
-					for(unsigned e = 0; e < per16; ++e) {
-						V &t = tile[psm + i * gstep + e];
-						t = vmul(t, diag_phase(dctx, hc & diag_hits(dctx, x0 + i * g.istride + e, vary, true)));
-					}
-				__syncthreads();
-			}
-		}
 		for(unsigned st = 0; st < nrun; ++st) {
 			const QftStage &S = sst[st];
 			const V *frow = ftab + (size_t)(S.fl == kQftNone ? 0u : S.fl) * nthr + tid;
 			const bool last = st + 1 == g.nstages;
 			qft_stage_dispatch<V, RB>(tile, S, spst[st * nthr + tid], frow, nthr, ot, s, g.roots,
-			                          last && direct ? a + tbase + slast : nullptr, nullptr);
+			                          last && direct ? a + tbase + slast : nullptr);
 			if(!(last && direct)) __syncthreads();
 			// Past the first stage's barrier every thread is done with the
 			// previous tile's buffer: the next copies go there.  (A pass of one
@@ -674,15 +563,13 @@ __global__ void __launch_bounds__(qft_max_threads(sizeof(typename Vec2<R>::type)
 			}
 		}
 		if(tail) {
-			const DiagCtx<V> *tdc = DG && g.dside == 2 ? &dctx : nullptr;
-			V *mdst = DG && mirror ? mirror + tbase : nullptr;
 			switch(sst[g.nstages - 1].d) {
-				case 1: wtail ? qft_tail<V, 1, true>(tile, a + tbase, T, tid, nthr, g, s, tdc, tbase, mdst)
-				              : qft_tail<V, 1, false>(tile, a + tbase, T, tid, nthr, g, s, tdc, tbase, mdst); break;
-				case 2: wtail ? qft_tail<V, 2, true>(tile, a + tbase, T, tid, nthr, g, s, tdc, tbase, mdst)
-				              : qft_tail<V, 2, false>(tile, a + tbase, T, tid, nthr, g, s, tdc, tbase, mdst); break;
-				case 3: wtail ? qft_tail<V, 3, true>(tile, a + tbase, T, tid, nthr, g, s, tdc, tbase, mdst)
-				              : qft_tail<V, 3, false>(tile, a + tbase, T, tid, nthr, g, s, tdc, tbase, mdst); break;
+				case 1: wtail ? qft_tail<V, 1, true>(tile, a + tbase, T, tid, nthr, g, s)
+				              : qft_tail<V, 1, false>(tile, a + tbase, T, tid, nthr, g, s); break;
+				case 2: wtail ? qft_tail<V, 2, true>(tile, a + tbase, T, tid, nthr, g, s)
+				              : qft_tail<V, 2, false>(tile, a + tbase, T, tid, nthr, g, s); break;
+				case 3: wtail ? qft_tail<V, 3, true>(tile, a + tbase, T, tid, nthr, g, s)
+				              : qft_tail<V, 3, false>(tile, a + tbase, T, tid, nthr, g, s); break;
 				default: break;
 			}
 		} else if(!direct) {
@@ -761,43 +648,21 @@ bool qft_segment(const FusedPass &pass, std::vector<unsigned> &hb, unsigned &r0)
 // Hadamards only, on two or more distinct local bits (a Walsh-Hadamard
 // segment: the Hadamards commute, so hb is any order of their bits; here
 // descending, as in a QFT segment).
-// Diagonal ops before (side 1) or after (side 2) the Hadamards of a Walsh
-// segment.
-struct WalshDiag {
-	unsigned side = 0;
-	std::vector<uint64_t> mask;
-	std::vector<double> cr, ci;
-	uint32_t flips = 0;
-};
-
-// Optionally with controlled phases and phase flips all before or all after
-// the Hadamards (at most kQftMaxDiag; they commute with one another).
-bool walsh_segment(const FusedPass &pass, std::vector<unsigned> &hb, WalshDiag &d) {
+// Hadamards only, on two or more distinct local bits (a Walsh-Hadamard
+// segment: the Hadamards commute, so hb is any order of their bits; here
+// descending, as in a QFT segment).
+bool walsh_segment(const FusedPass &pass, std::vector<unsigned> &hb) {
 	hb.clear();
-	d = WalshDiag{};
 	uint64_t seen = 0;
-	unsigned before = 0, after = 0;
 	for(const FusedOp &f : pass.ops) {
-		if(f.kind == kFCP || f.kind == kFFlip) {
-			if(d.mask.size() == kQftMaxDiag) return false;
-			if(hb.empty()) ++before;
-			else ++after;
-			if(f.kind == kFFlip) d.flips |= 1u << d.mask.size();
-			d.mask.push_back(f.kind == kFCP ? f.mask : f.state);
-			d.cr.push_back(f.kind == kFCP ? f.cr : -1.0);
-			d.ci.push_back(f.kind == kFCP ? f.ci : 0.0);
-			continue;
-		}
-		if(f.kind != kFH || f.lt >= pass.K || after) return false;  // Hadamards in one run
+		if(f.kind != kFH || f.lt >= pass.K) return false;
 		const unsigned b = pass.lpos[f.lt];
 		if((seen >> b) & 1ull) return false;
 		seen |= 1ull << b;
 		hb.push_back(b);
 	}
-	if(before && after) return false;
-	d.side = before ? 1u : (after ? 2u : 0u);
 	std::sort(hb.begin(), hb.end(), [](unsigned x, unsigned y) { return x > y; });
-	return hb.size() >= (d.side ? 1u : 2u);
+	return hb.size() >= 2;
 }
 
 inline unsigned insert_zeros(unsigned t, const uint32_t *sorted, int count) {
@@ -820,7 +685,7 @@ struct Swizzle {
 
 // Plans the pass for storage values of vbytes bytes and RB register bits.
 bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r0, unsigned vbytes, unsigned RB,
-              QftGeom &g, bool walsh, bool allow_tma = false, const WalshDiag *diag = nullptr) {
+              QftGeom &g, bool walsh, bool allow_tma = false) {
 	const unsigned K = pass.K, n = pass.n, per16 = 16 / vbytes;
 	const unsigned lgran = RB - (per16 == 2 ? 1u : 0u);  // log2 of the granules per thread
 	if(K > 14 || K < RB + 5 || (1u << (K - RB)) > qft_max_threads(vbytes, (int)RB)) return false;
@@ -1054,21 +919,6 @@ bool plan_qft(const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r
 		b = e;
 	}
 	g.scale = std::ldexp((np & 1u) ? 1.0 / std::sqrt(2.0) : 1.0, -(int)(np / 2));
-	g.dside = 0;
-	if(diag && diag->side) {
-		// After the Hadamards: applied where the tile leaves, in the fused tail.
-		if(diag->side == 2 && !g.st[nst - 1].tail) return false;
-		g.dside = diag->side;
-		g.dcount = (unsigned)diag->mask.size();
-		g.dbytes = (n + 7) / 8;
-		g.dgroups = (g.dcount + 7) / 8;
-		g.dflip = diag->flips;
-		for(unsigned k = 0; k < g.dcount; ++k) {
-			g.dmask[k] = diag->mask[k];
-			g.dcr[k] = diag->cr[k];
-			g.dci[k] = diag->ci[k];
-		}
-	}
 	return true;
 }
 
@@ -1112,18 +962,15 @@ bool encode_tile_map(CUtensorMap &m, void *a, const QftGeom &g) {
 #ifndef TMFQS_QFT_PLAN_ONLY  // (host checks of the planner compile without the kernels)
 template <typename R, int RB>
 bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass, const std::vector<unsigned> &hb, unsigned r0,
-             bool walsh, const WalshDiag &diag, void *mirror) {
+             bool walsh) {
 	typedef typename Vec2<R>::type V;
 	QftGeom g;
-	if(!c.err || !plan_qft(pass, hb, r0, (unsigned)sizeof(V), (unsigned)RB, g, walsh, true, &diag)) return false;
-	// A checkpoint copy of the result is written by the fused tail only.
-	if(mirror && !g.st[g.nstages - 1].tail) return false;
+	if(!c.err || !plan_qft(pass, hb, r0, (unsigned)sizeof(V), (unsigned)RB, g, walsh, sizeof(V) == 8)) return false;
 	const unsigned nthr = 1u << (g.K - RB);
 	const size_t T = size_t(1) << g.K;
 	auto smem_for = [&](unsigned slots) {
 		return (slots * T + (size_t)g.nfrows * nthr + (size_t)slots * g.ot_stride) * sizeof(V) +
-		       kQftMaxStages * sizeof(QftStage) + slots * 8 + (size_t)g.nstages * nthr * 2 + (g.tma ? 1024 : 0) +
-		       (g.dside ? 16 + (size_t)g.dbytes * 256 * 4 + (size_t)g.dgroups * 256 * sizeof(V) : 0);
+		       kQftMaxStages * sizeof(QftStage) + slots * 8 + (size_t)g.nstages * nthr * 2 + (g.tma ? 1024 : 0);
 	};
 	int dev = 0, max_optin = 0;
 	check_cuda(cudaGetDevice(&dev), "qft device");
@@ -1134,40 +981,57 @@ bool run_qft(const LaunchCtx &c, void *a, const FusedPass &pass, const std::vect
 	CUtensorMap tmap;
 	std::memset(&tmap, 0, sizeof(tmap));
 	if(g.tma && !encode_tile_map(tmap, a, g)) g.tma = 0;  // no encoder: per-thread copies (same swizzle)
-	// Diagonal tables and checkpoint copies (DG) only where needed, so that
-	// the other passes keep their register budget.
-	const bool dg = g.dside || mirror;
-	auto kern = g.tma ? (dg ? k_qft_pass<R, RB, true, true> : k_qft_pass<R, RB, true, false>)
-	                  : (dg ? k_qft_pass<R, RB, false, true> : k_qft_pass<R, RB, false, false>);
+	void (*kern)(V *, const QftGeom, const CUtensorMap, int *) = k_qft_pass<R, RB, false>;
+	if constexpr(sizeof(V) == 8) {  // tensor-map tiles: complex64 only
+		if(g.tma) kern = k_qft_pass<R, RB, true>;
+	}
 	check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "qft smem");
 	const uint64_t grid = std::min<uint64_t>(g.ntiles, (uint64_t)c.num_sms);
-	kern<<<(unsigned)grid, nthr, smem, c.stream>>>(static_cast<V *>(a), g, tmap, static_cast<V *>(mirror), c.err);
+	kern<<<(unsigned)grid, nthr, smem, c.stream>>>(static_cast<V *>(a), g, tmap, c.err);
 	check_cuda(cudaGetLastError(), "qft pass");
 	if(c.launches) ++*c.launches;
 	return true;
 }
 
+// One precision's launcher (recognition, plan, launch).
+template <typename R, int RB>
+bool launch_qft_pass_for(const LaunchCtx &c, void *a, const FusedPass &pass, bool allow_walsh) {
+	std::vector<unsigned> hb;
+	unsigned r0 = 0;
+	bool walsh = false;
+	if(!qft_segment(pass, hb, r0)) {
+		if(!allow_walsh || !walsh_segment(pass, hb)) return false;
+		walsh = true;
+		r0 = pass.n;  // no phases: no twiddle range
+	}
+	return run_qft<R, RB>(c, a, pass, hb, r0, walsh);
+}
 #endif
 
 }  // namespace
 
+// The kernels of each precision are compiled in their own unit
+// (qft_pass_c64.cu, qft_pass_c128.cu, which include this file), so that the
+// two build in parallel; this unit holds the dispatch.
 #ifndef TMFQS_QFT_PLAN_ONLY
-bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, bool allow_walsh, void *mirror) {
-	std::vector<unsigned> hb;
-	unsigned r0 = 0;
-	bool walsh = false;
-	WalshDiag diag;
-	if(!qft_segment(pass, hb, r0)) {
-		if(!allow_walsh || !walsh_segment(pass, hb, diag)) return false;
-		walsh = true;
-		r0 = pass.n;  // no twiddles
-	}
-	if(prec == TMFQS_FP64) return run_qft<double, 4>(c, a, pass, hb, r0, walsh, diag, mirror);
-	// complex64: 5-bit stages (256 threads).  4-bit stages with 512 threads
-	// measured the same at 28 and 30 qubits and 2% slower at 26 with one
-	// barrier per tile.
-	return run_qft<float, 5>(c, a, pass, hb, r0, walsh, diag, mirror);
+#if defined(TMFQS_QFT_UNIT_C64)
+// complex64: 5-bit stages (256 threads).  4-bit stages with 512 threads
+// measured the same at 28 and 30 qubits and 2% slower at 26 with one barrier
+// per tile.
+bool launch_qft_pass_c64(const LaunchCtx &c, void *a, const FusedPass &pass, bool allow_walsh) {
+	return launch_qft_pass_for<float, 5>(c, a, pass, allow_walsh);
 }
+#elif defined(TMFQS_QFT_UNIT_C128)
+bool launch_qft_pass_c128(const LaunchCtx &c, void *a, const FusedPass &pass, bool allow_walsh) {
+	return launch_qft_pass_for<double, 4>(c, a, pass, allow_walsh);
+}
+#else
+bool launch_qft_pass_c64(const LaunchCtx &c, void *a, const FusedPass &pass, bool allow_walsh);
+bool launch_qft_pass_c128(const LaunchCtx &c, void *a, const FusedPass &pass, bool allow_walsh);
+bool launch_qft_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, bool allow_walsh) {
+	return prec == TMFQS_FP64 ? launch_qft_pass_c128(c, a, pass, allow_walsh) : launch_qft_pass_c64(c, a, pass, allow_walsh);
+}
+#endif
 #endif
 
 }  // namespace tqb
