@@ -1002,6 +1002,7 @@ struct StageGeom {
 	uint8_t op_reg[kStMaxOps];                     // register bit of the op's Hadamard
 	uint16_t op_tab[kStMaxOps], op_lc[kStMaxOps];  // its chain: entries [tab, tab + lc) of the pass
 	uint8_t op_split[kStMaxOps];                   // entries from here on have no register-bit control
+	uint8_t op_outer[kStMaxOps];                   // the chain has entries controlled by outer bits
 	uint8_t scol[kStK];                            // shared slot of j: j ^ XOR of scol[b] over bits b >= 3 of j
 };
 
@@ -1171,7 +1172,7 @@ __device__ __forceinline__ void stage_hchain(typename Vec2<R>::type (&v)[16], R 
 	// The entries whose control is an outer bit set in this tile (one lane per
 	// entry, the same in every warp).
 	uint64_t cu = 0;
-	{
+	if(g.op_outer[k]) {
 		const unsigned lane = t & 31u, tb = g.op_tab[k], lc = g.op_lc[k];
 		for(unsigned e0 = 0; e0 < lc; e0 += 32) {
 			const unsigned e = e0 + lane;
@@ -1528,7 +1529,10 @@ bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phas
 		for(unsigned e = 0; e < lc; ++e) {
 			const ChainEntry &ce = pass.chain[op.tab + e];
 			phases.push_back(double2{ce.cr, ce.ci});
-			if(ce.local < 0) continue;
+			if(ce.local < 0) {
+				g.op_outer[k] = 1;
+				continue;
+			}
 			const uint64_t bit = 1ull << (63 - e);
 			bool reg = false;
 			for(unsigned i = 0; i < kStRB; ++i)
