@@ -186,6 +186,9 @@ static void check_stages(const char *name, const FusedPass &p) {
 		for(unsigned k = g.st_first[st]; k < g.st_first[st] + g.st_count[st]; ++k) {
 			const FusedOp &op = p.ops[k];
 			EXPECT(g.rbit[st][g.op_reg[k]] == op.lt, "%s op %u: target is not its register bit", name, k);
+			bool outer = false;
+			for(unsigned e = 0; e < op.lc; ++e) outer = outer || p.chain[op.tab + e].local < 0;
+			EXPECT((g.op_outer[k] != 0) == outer, "%s op %u: outer-control flag", name, k);
 			const uint64_t *Tb = tab.data() + (size_t)k * kStTabWords;
 			const unsigned I = g.op_reg[k];
 			uint64_t rall = 0;
