@@ -209,15 +209,17 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 		V lb[kGradBatch], pb[kGradBatch];
 		if constexpr(sizeof(V) == 8) {
 			if(lim == kGradBatch) {
-				// Eight complex64 values: four 16-byte loads each (x0 is a multiple of 8).
-				const float4 *l4 = reinterpret_cast<const float4 *>(lam + x0), *p4 = reinterpret_cast<const float4 *>(psi + x0);
+				// Eight complex64 values: two 32-byte loads each (x0 is a multiple of 8).
 #pragma unroll
-				for(unsigned q = 0; q < kGradBatch / 2; ++q) {
-					const float4 a = l4[q], b = p4[q];
-					lb[2 * q] = V{a.x, a.y};
-					lb[2 * q + 1] = V{a.z, a.w};
-					pb[2 * q] = V{b.x, b.y};
-					pb[2 * q + 1] = V{b.z, b.w};
+				for(unsigned q = 0; q < kGradBatch / 4; ++q) {
+					float a[8], b[8];
+					ld_global_v8f(reinterpret_cast<const float *>(lam + x0 + 4 * q), a);
+					ld_global_v8f(reinterpret_cast<const float *>(psi + x0 + 4 * q), b);
+#pragma unroll
+					for(unsigned u = 0; u < 4; ++u) {
+						lb[4 * q + u] = V{a[2 * u], a[2 * u + 1]};
+						pb[4 * q + u] = V{b[2 * u], b[2 * u + 1]};
+					}
 				}
 			}
 		}
@@ -268,11 +270,18 @@ __global__ void __launch_bounds__(kAdjThreads, 2) k_grad_run(typename Vec2<R>::t
 		}
 		if constexpr(sizeof(V) == 8) {
 			if(lim == kGradBatch) {
-				float4 *l4 = reinterpret_cast<float4 *>(lam + x0), *p4 = reinterpret_cast<float4 *>(psi + x0);
 #pragma unroll
-				for(unsigned q = 0; q < kGradBatch / 2; ++q) {
-					l4[q] = make_float4(lo[2 * q].x, lo[2 * q].y, lo[2 * q + 1].x, lo[2 * q + 1].y);
-					if(uncompute_psi) p4[q] = make_float4(po[2 * q].x, po[2 * q].y, po[2 * q + 1].x, po[2 * q + 1].y);
+				for(unsigned q = 0; q < kGradBatch / 4; ++q) {
+					float a[8], b[8];
+#pragma unroll
+					for(unsigned u = 0; u < 4; ++u) {
+						a[2 * u] = lo[4 * q + u].x;
+						a[2 * u + 1] = lo[4 * q + u].y;
+						b[2 * u] = po[4 * q + u].x;
+						b[2 * u + 1] = po[4 * q + u].y;
+					}
+					st_global_v8f(reinterpret_cast<float *>(lam + x0 + 4 * q), a);
+					if(uncompute_psi) st_global_v8f(reinterpret_cast<float *>(psi + x0 + 4 * q), b);
 				}
 			}
 		}

@@ -57,6 +57,18 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 	const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
 	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+// 32-byte global loads and stores (sm_100 vector width; 32-byte aligned).
+__device__ __forceinline__ void ld_global_v8f(const float *p, float (&r)[8]) {
+	asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+	             : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7])
+	             : "l"(p));
+}
+__device__ __forceinline__ void st_global_v8f(float *p, const float (&r)[8]) {
+	asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(r[0]), "f"(r[1]), "f"(r[2]),
+	             "f"(r[3]), "f"(r[4]), "f"(r[5]), "f"(r[6]), "f"(r[7])
+	             : "memory");
+}
+
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
