@@ -1241,6 +1241,9 @@ void load_apply_ops_body(tmfqs_gpu_state *h, unsigned n, const double *host, con
 	h->initialized = true;
 	h->cur_first = 0;
 	h->cur_count = (unsigned)k;
+	// The slabs' launches share one program: upload it now, ahead of the slab
+	// copies (on the same copy engine a later upload would queue behind them).
+	fp.program_ready = tqb::prepare_fused_pass(ctx(h), h->precision, fp, h->dev_prog, h->dev_prog_bytes);
 	const uint64_t per = (1ull << (nout - t));
 	for(unsigned v = 0; v < slabs; ++v) {
 		unsigned char *dst = static_cast<unsigned char *>(h->amps) + (size_t(v) << pbit) * 16;

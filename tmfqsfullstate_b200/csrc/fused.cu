@@ -1562,7 +1562,8 @@ bool plan_stages(const FusedPass &pass, StageGeom &g, std::vector<double2> &phas
 }
 
 template <typename R>
-bool run_fused_stages(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_prog, size_t &dev_prog_bytes) {
+bool run_fused_stages(const LaunchCtx &c, void *a, const FusedPass &pass, void *&dev_prog, size_t &dev_prog_bytes,
+                      bool upload_only = false) {
 	StageGeom g;
 	std::vector<double2> phases;
 	std::vector<uint64_t> tab;
@@ -1578,24 +1579,29 @@ bool run_fused_stages(const LaunchCtx &c, void *a, const FusedPass &pass, void *
 	const size_t ph_off = (ch_bytes + 255) & ~size_t(255);
 	const size_t tab_off = (ph_off + std::max<size_t>(16, phases.size() * sizeof(double2)) + 255) & ~size_t(255);
 	const size_t need = tab_off + tab.size() * sizeof(uint64_t);
-	if(need > dev_prog_bytes) {
-		if(dev_prog) {
-			check_cuda(cudaStreamSynchronize(c.stream), "fused program sync");
-			cudaFree(dev_prog);
+	if(pass.program_ready) {
+		if(need > dev_prog_bytes) fail(TMFQS_ERR_LOGIC, "fused pass: prepared program missing");
+	} else {
+		if(need > dev_prog_bytes) {
+			if(dev_prog) {
+				check_cuda(cudaStreamSynchronize(c.stream), "fused program sync");
+				cudaFree(dev_prog);
+			}
+			dev_prog = nullptr;
+			dev_prog_bytes = 0;
+			if(device_alloc(&dev_prog, need * 2) != cudaSuccess) {
+				cudaGetLastError();
+				fail(TMFQS_ERR_NOMEM, "fused pass program allocation failed");
+			}
+			dev_prog_bytes = need * 2;
 		}
-		dev_prog = nullptr;
-		dev_prog_bytes = 0;
-		if(device_alloc(&dev_prog, need * 2) != cudaSuccess) {
-			cudaGetLastError();
-			fail(TMFQS_ERR_NOMEM, "fused pass program allocation failed");
-		}
-		dev_prog_bytes = need * 2;
+		std::vector<unsigned char> host(need, 0);
+		if(!pass.chain.empty()) std::memcpy(host.data(), pass.chain.data(), pass.chain.size() * sizeof(ChainEntry));
+		if(!phases.empty()) std::memcpy(host.data() + ph_off, phases.data(), phases.size() * sizeof(double2));
+		std::memcpy(host.data() + tab_off, tab.data(), tab.size() * sizeof(uint64_t));
+		upload_async(c, dev_prog, host.data(), need, "fused program upload");
 	}
-	std::vector<unsigned char> host(need, 0);
-	if(!pass.chain.empty()) std::memcpy(host.data(), pass.chain.data(), pass.chain.size() * sizeof(ChainEntry));
-	if(!phases.empty()) std::memcpy(host.data() + ph_off, phases.data(), phases.size() * sizeof(double2));
-	std::memcpy(host.data() + tab_off, tab.data(), tab.size() * sizeof(uint64_t));
-	upload_async(c, dev_prog, host.data(), need, "fused program upload");
+	if(upload_only) return true;
 	unsigned char *dp = static_cast<unsigned char *>(dev_prog);
 	const size_t smem = stage_smem_layout(sizeof(typename Vec2<R>::type), g.m, g.nops, g.nentries, g.nstages).total;
 	auto kern = g.narrow ? k_fused_stages<R, true> : k_fused_stages<R, false>;
@@ -1611,6 +1617,11 @@ bool run_fused_stages(const LaunchCtx &c, void *a, const FusedPass &pass, void *
 }
 
 }  // namespace
+
+bool prepare_fused_pass(const LaunchCtx &c, int prec, const FusedPass &pass, void *&dev_prog, size_t &dev_prog_bytes) {
+	if(prec != TMFQS_FP64 || pass.program_ready) return false;
+	return run_fused_stages<double>(c, nullptr, pass, dev_prog, dev_prog_bytes, true);
+}
 
 void launch_fused_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, void *&dev_prog,
                        size_t &dev_prog_bytes) {

@@ -166,12 +166,20 @@ struct FusedPass {
 	unsigned gate_count = 0;        // circuit operations folded into this pass
 	// Exact fused passes: run only tiles [tile_begin, tile_end) (0, 0: all).
 	uint64_t tile_begin = 0, tile_end = 0;
+	// The pass's program is already in `dev_prog` (prepare_fused_pass): the
+	// launch uploads nothing.
+	bool program_ready = false;
 };
 
 // Runs one fused pass over the whole state.  `dev_prog` is a device buffer
 // the launcher may (re)use for the program.
 void launch_fused_pass(const LaunchCtx &c, int prec, void *a, const FusedPass &pass, void *&dev_prog,
                        size_t &dev_prog_bytes);
+
+// Uploads the program of an exact register-stage pass into `dev_prog` ahead
+// of its launches (the tile ranges of one pass share it); false when the pass
+// runs another kernel (which uploads at launch).
+bool prepare_fused_pass(const LaunchCtx &c, int prec, const FusedPass &pass, void *&dev_prog, size_t &dev_prog_bytes);
 
 // Radix-2^RB form of a fused pass for the fast forms (complex64, or complex128
 // without exact arithmetic): programs of H, H-chains, twiddles and controlled
