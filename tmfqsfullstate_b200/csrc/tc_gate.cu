@@ -68,17 +68,6 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t da, uint64_t db
 		::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
-// Eight TMEM columns of this thread's lane.
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
-	uint32_t r[8];
-	asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-	             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-	             : "r"(taddr));
-	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-	for(int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
-}
-
 // Sixteen TMEM columns of this thread's lane, without waiting (the caller
 // waits once for a batch of these with tmem_wait_ld).
 __device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&r)[16]) {
